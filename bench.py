@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""D3Q19 wind-tunnel step throughput on B200 (MLUPS and fraction of the HBM roofline).
+
+Workload (default): the D3Q19 TRT tunnel at 192x96x96 with FP32 storage, a sphere of diameter 16
+at (48, 48, 48) as an SDF with Bouzidi walls, equilibrium inlet ramped linearly to u = 0.1 over
+3000 steps (device-side ramp), copy-and-relax outlet, slip side faces, outlet sponge over the last
+15% with absorb 0.02, Re 200 (tau = 0.524, Lambda = 50 (tau - 1/2)^2), start from rest with a seeded
+1e-4 velocity perturbation, forces sampled every step. Inputs are synthetic (seed 20261203).
+
+One step = one fused step kernel over the whole grid. The two distribution buffers (2 x 134 MB)
+exceed the 126 MB L2, so every timed step streams from HBM without an explicit flush.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N under torchrun every rank runs an independent replica on its own GPU (the path does
+not shard: replicas only); value is the whole-job MLUPS from the max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "D3Q19 MLUPS + % HBM peak, FP16 vs FP32 store at C_D err≤1%; adjoint cost/fwd"
+BYTES_PER_CELL = {"fp32": 152, "fp16": 76, "bf16": 76, "fp64": 304}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(workload: str):
+    """dram bytes per launch of the step kernel from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(workload)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu), "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def physical_gpu_index(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local_rank < len(ids) and ids[local_rank].isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+# ---------------------------------------------------------------- workload
+
+
+def tunnel_setup(W, H, D, precision, device, tau=None, exact=False):
+    from cells_b200 import Solver3D, geometry as g
+    from cells_b200.rng import perturbed_rest3
+    from cells_b200.units import derive_tau
+
+    d = 16 * H / 96  # sphere diameter 16 on the 96-high grid; scaled with the grid
+    tau = derive_tau(200, 0.1, d).tau if tau is None else tau
+    s = Solver3D.create(W, H, D, precision=precision, tau=tau, uIn=0.0, spongeFraction=0.15, spongeTau=1.0,
+                        absorb=0.02, forceEvery=1, device=device, exactArithmetic=exact)
+    sdf = g.empty_sdf3(W, H, D)
+    g.add_sphere(sdf, W, H, D, W / 4, H / 2, D / 2, d / 2)
+    macro = perturbed_rest3(W, H, D, 1e-4)
+    return s, sdf, macro, tau
+
+
+def time_steps(s, warmup: int, steps: int):
+    s.encodeSteps(warmup)
+    s.synchronize()
+    s.readForces()
+    l0 = s.launchCount()
+    s.timerStart()
+    s.encodeSteps(steps)
+    ms = s.timerStop()
+    launches = s.launchCount() - l0
+    s.readForces()
+    return ms, launches
+
+
+def run_e2e(s, sdf, macro, steps: int, chunk: int = 100):
+    """The reference's caller pattern (src/cases.ts:41-59) through the public API with host buffers:
+    setSdf and initField from host arrays, then per chunk setInlet (host-ramped), run(chunk) and
+    readForces, and readMacro at the end. Wall clock, synchronised on the device."""
+    import numpy as np
+
+    s.synchronize()
+    h2d = d2h = 0
+    t0 = time.perf_counter()
+    s.setSdf(sdf)
+    h2d += sdf.nbytes
+    s.initField(macro)
+    h2d += macro.nbytes
+    forces = 0
+    done = 0
+    while done < steps:
+        k = min(chunk, steps - done)
+        t = min(1.0, done / 3000)
+        s.setInlet(0.1 * t)
+        h2d += 8
+        s.run(k, k)
+        f = s.readForcesArray()
+        forces += len(f)
+        d2h += 32 * len(f)
+        done += k
+    m = s.readMacro()
+    d2h += m.nbytes
+    dt = time.perf_counter() - t0
+    assert np.all(np.isfinite(m))
+    return dt, h2d, d2h
+
+
+def cpu_baseline(W, H, D, precision="fp32", budget_s=12.0, max_steps=400):
+    """The oracle (C++ restatement of the reference's kernels) on the host cores, OpenMP."""
+    from cells_b200 import geometry as g
+    from cells_b200.rng import perturbed_rest3
+    from cells_b200.units import derive_tau
+    from oracle.oracle import OracleSolver3D, lib as olib
+
+    d = 16 * H / 96
+    tau = derive_tau(200, 0.1, d).tau
+    o = OracleSolver3D(W, H, D, precision, tau=tau, uIn=0.0, spongeFraction=0.15, absorb=0.02, forceEvery=1)
+    sdf = g.empty_sdf3(W, H, D)
+    g.add_sphere(sdf, W, H, D, W / 4, H / 2, D / 2, d / 2)
+    o.setSdf(sdf)
+    o.initField(perturbed_rest3(W, H, D, 1e-4))
+    o.setInlet(0.1)
+    t0 = time.perf_counter()
+    o.encodeSteps(1)
+    one = time.perf_counter() - t0
+    k = max(1, min(max_steps, int(budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    o.encodeSteps(k)
+    dt = time.perf_counter() - t0
+    N = W * H * D
+    return {"value": N * k / dt / 1e6, "unit": "MLUPS", "cores": int(olib().oracle_num_threads()), "kind": "port",
+            "sample": f"{k} full D3Q19 steps of the {W}x{H}x{D} {precision} sphere tunnel on the CPU oracle "
+                      f"(OpenMP), {dt:.1f} s"}
+
+
+# ---------------------------------------------------------------- main
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32")
+    ap.add_argument("--grid", default="192x96x96")
+    ap.add_argument("--no-extras", action="store_true", help="skip e2e, variants and the CPU baseline")
+    ap.add_argument("--profile", action="store_true", help="short run for ncu: warmup + steps only, no extras")
+    args = ap.parse_args()
+    W, H, D = (int(v) for v in args.grid.lower().split("x"))
+    N = W * H * D
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # plumbing only: a barrier and a max over ranks
+        from datetime import timedelta
+
+        dist.init_process_group(backend="gloo", timeout=timedelta(seconds=120))
+    workload = f"D3Q19 {W}x{H}x{D} {args.precision} sphere d=16 Re200 tunnel"
+
+    if args.impl == "reference":
+        if rank == 0:
+            cb = cpu_baseline(W, H, D, args.precision, budget_s=60.0, max_steps=max(1, args.steps))
+            line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "MLUPS", "n_gpus": args.gpus,
+                    "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                    "config": {"workload": workload, "grid": [W, H, D], "storage": args.precision,
+                               "note": "the reference is TypeScript+WGSL for browser WebGPU, which cannot run here; "
+                                       "its kernels' C++ restatement (oracle/) runs on the host cores instead"},
+                    "cpu_baseline": cb,
+                    "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    from cells_b200 import analysis
+
+    s, sdf, macro, tau = tunnel_setup(W, H, D, args.precision, device=local)
+    s.setSdf(sdf)
+    s.initField(macro)
+    s.setInletRamp("linear", 0.1, 3000, 1)
+    if dist is not None:
+        dist.barrier()
+    with ClockSampler(physical_gpu_index(local)) as clocks:
+        ms, launches = time_steps(s, max(3, args.warmup), args.steps)
+    clk = clocks.summary()
+    if dist is not None:
+        import torch
+
+        t = torch.tensor([ms], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    mlups = world * N * args.steps / (ms * 1e3)
+    per_gpu_mlups = N * args.steps / (ms * 1e3)
+    hbm, peak_kind = peaks()
+    achieved = per_gpu_mlups * 1e6 * BYTES_PER_CELL[args.precision] / 1e9
+    traffic = profiled_traffic(workload)
+    info = s.info()
+    line = {
+        "metric": METRIC, "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if args.precision != "fp64" else "f64", "data": "synthetic",
+        "config": {"workload": workload, "grid": [W, H, D], "storage": args.precision, "tau": tau,
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (2 x 134 MB populations)",
+                   "block": [info["block_x"], info["block_y"]], "force_blocks": info["n_force_blocks"]},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": peak_kind,
+                     "bytes_per_cell": BYTES_PER_CELL[args.precision]},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if not args.no_extras and not args.profile:
+        e2e_steps = min(args.steps, 1000)
+        dt, h2d, d2h = run_e2e(s, sdf, macro, e2e_steps)
+        line["e2e"] = {"value": round(N * e2e_steps / dt / 1e6 * world, 1), "unit": "MLUPS",
+                       "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
+                       "steps": e2e_steps, "calls": "setSdf, initField, (setInlet, run(100), readForces) x k, readMacro"}
+        f = s.readForcesArray()
+        s.destroy()
+        variants = []
+        for prec, grid in (("fp16", (W, H, D)), ("bf16", (W, H, D)), ("fp64", (W, H, D)),
+                           ("fp32", (256, 128, 128)), ("fp16", (256, 128, 128))):
+            v, vsdf, vmac, _ = tunnel_setup(*grid, prec, device=local)
+            v.setSdf(vsdf)
+            v.initField(vmac)
+            v.setInletRamp("linear", 0.1, 3000, 1)
+            vms, _ = time_steps(v, 50, 500)
+            vn = grid[0] * grid[1] * grid[2]
+            vm = vn * 500 / (vms * 1e3)
+            variants.append({"storage": prec, "grid": list(grid), "mlups": round(vm, 1),
+                             "hbm_frac": round(vm * 1e6 * BYTES_PER_CELL[prec] / 1e9 / hbm, 4)})
+            v.destroy()
+        line["variants"] = variants
+        if rank == 0 and world == 1:
+            line["cpu_baseline"] = cpu_baseline(W, H, D, args.precision)
+    else:
+        s.destroy()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,130 @@
+"""ctypes binding of libcells.so (the C ABI declared in include/cells.h).
+
+The library is built in-tree (``cells_b200/libcells.so``) by ``__graft_entry__.build()``. There is
+no fallback: importing a solver without the built library raises, so a missing extension can never
+silently turn into a CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcells.so")
+
+CELLS_OK = 0
+CELLS_E_ALLOC = 1
+CELLS_E_PRECISION_UNSUPPORTED = 2
+CELLS_E_INVALID = 3
+CELLS_E_CUDA = 4
+CELLS_E_DIVERGED = 5
+CELLS_E_TIMEOUT = 6
+
+FP32, FP16, BF16, FP64 = 0, 1, 2, 3
+PRECISIONS = {"fp32": FP32, "fp16": FP16, "bf16": BF16, "fp64": FP64}
+BYTES_PER_POPULATION = {FP32: 4, FP16: 2, BF16: 2, FP64: 8}
+FAKE_DEVICE = -2
+RAMP_NONE, RAMP_LINEAR, RAMP_SMOOTHSTEP = 0, 1, 2
+ARITH_FAST, ARITH_EXACT = 0, 1
+
+
+class Cells3DConfig(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32), ("height", C.c_int32), ("depth", C.c_int32), ("precision", C.c_int32),
+        ("tau", C.c_double), ("lambda_", C.c_double), ("smagorinsky", C.c_double), ("u_in", C.c_double),
+        ("sponge_fraction", C.c_double), ("sponge_tau", C.c_double), ("absorb", C.c_double),
+        ("workgroup_size", C.c_int32), ("force_every", C.c_int32), ("device", C.c_int32),
+        ("fake_fail_alloc", C.c_int32), ("max_buffer_bytes", C.c_uint64), ("arithmetic", C.c_int32),
+        ("reserved1", C.c_int32),
+    ]
+
+
+class CellsForceSample(C.Structure):
+    _fields_ = [("step", C.c_uint32), ("reserved", C.c_uint32), ("fx", C.c_double), ("fy", C.c_double),
+                ("fz", C.c_double)]
+
+
+class Cells3DInfo(C.Structure):
+    _fields_ = [
+        ("W", C.c_int32), ("H", C.c_int32), ("D", C.c_int32), ("precision", C.c_int32),
+        ("N", C.c_int64), ("step", C.c_int64), ("block_x", C.c_int32), ("block_y", C.c_int32),
+        ("force_every", C.c_int32), ("n_force_blocks", C.c_int32),
+    ]
+
+
+class CellsError(RuntimeError):
+    """A failed libcells call: ``status`` is the cells_status code, the message is the library's."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run __graft_entry__.build() (make -C cells_b200/csrc)")
+    L = C.CDLL(LIB_PATH)
+    P, I, D, I64, SZ = C.c_void_p, C.c_int, C.c_double, C.c_int64, C.c_size_t
+    sig = {
+        "cells3d_config_default": (None, [C.POINTER(Cells3DConfig)]),
+        "cells3d_create": (I, [C.POINTER(Cells3DConfig), C.POINTER(P)]),
+        "cells3d_destroy": (None, [P]),
+        "cells_last_error": (C.c_char_p, [P]),
+        "cells3d_set_tau": (I, [P, D]),
+        "cells3d_set_smagorinsky": (I, [P, D]),
+        "cells3d_set_inlet": (I, [P, D]),
+        "cells3d_set_lambda": (I, [P, D]),
+        "cells3d_set_inlet_ramp": (I, [P, I, D, I64, I64]),
+        "cells3d_set_sdf": (I, [P, P, SZ]),
+        "cells3d_init_field": (I, [P, P]),
+        "cells3d_reset_forces": (I, [P]),
+        "cells3d_step": (I, [P, I64]),
+        "cells3d_update_macro": (I, [P]),
+        "cells3d_run": (I, [P, I64, I64]),
+        "cells3d_synchronize": (I, [P]),
+        "cells3d_read_macro": (I, [P, P]),
+        "cells3d_read_forces": (I, [P, C.POINTER(CellsForceSample), SZ, C.POINTER(SZ)]),
+        "cells3d_read_forces_begin": (I, [P]),
+        "cells3d_read_forces_end": (I, [P, C.POINTER(CellsForceSample), SZ, C.POINTER(SZ)]),
+        "cells3d_read_status": (I, [P, C.POINTER(C.c_uint32)]),
+        "cells3d_get_info": (I, [P, C.POINTER(Cells3DInfo)]),
+        "cells3d_read_params": (I, [P, P]),
+        "cells3d_mass": (I, [P, C.POINTER(D)]),
+        "cells3d_read_populations": (I, [P, P, SZ]),
+        "cells3d_write_populations": (I, [P, P, SZ]),
+        "cells3d_read_flags": (I, [P, P, SZ]),
+        "cells3d_timer_start": (I, [P]),
+        "cells3d_timer_stop": (I, [P, C.POINTER(C.c_float)]),
+        "cells3d_launch_count": (I, [P, C.POINTER(I64)]),
+        "cells3d_fake_set_force": (I, [P, D, D, D]),
+        "cells_fake_live_buffers": (I64, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status: int, handle=None) -> None:
+    if status != CELLS_OK:
+        msg = lib().cells_last_error(handle)
+        raise CellsError(status, msg.decode() if msg else f"libcells status {status}")
+
+
+def default_config3() -> Cells3DConfig:
+    c = Cells3DConfig()
+    lib().cells3d_config_default(C.byref(c))
+    return c
+
+
+def nan() -> float:
+    return math.nan

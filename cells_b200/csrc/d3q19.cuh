@@ -1,0 +1,112 @@
+// D3Q19 lattice constants, storage codecs and the shared device/host structures of the 3D engine.
+//
+// Lattice: src/lattice3d.ts:4-26 (velocity set with odd i and i+1 opposite, weights 1/3, 1/18, 1/36,
+// MIRROR_Y/Z, flag bits 19-21). Codec: src/shaders/common3d.ts:52-63 (f16 scaled by 2^15 and
+// clamped to +-1.99 before the store); bf16 and f64 are additions of this engine.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cells {
+
+constexpr int Q3 = 19;
+constexpr uint32_t FLAG3_SOLID = 1u << 19;
+constexpr uint32_t FLAG3_INLET = 1u << 20;
+constexpr uint32_t FLAG3_OUTLET = 1u << 21;
+constexpr int HISTORY_LEN = 8192;  // src/shaders/aux3d.ts:5
+
+__host__ __device__ __forceinline__ constexpr int cx3(int i) {
+  constexpr int v[Q3] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0};
+  return v[i];
+}
+__host__ __device__ __forceinline__ constexpr int cy3(int i) {
+  constexpr int v[Q3] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1};
+  return v[i];
+}
+__host__ __device__ __forceinline__ constexpr int cz3(int i) {
+  constexpr int v[Q3] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1};
+  return v[i];
+}
+__host__ __device__ __forceinline__ constexpr int opp3(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
+// Direction with its y (z) component negated, for slip on the y (z) faces.
+__host__ __device__ __forceinline__ constexpr int mirror_y3(int i) {
+  constexpr int v[Q3] = {0, 1, 2, 4, 3, 5, 6, 13, 14, 9, 10, 18, 17, 7, 8, 15, 16, 12, 11};
+  return v[i];
+}
+__host__ __device__ __forceinline__ constexpr int mirror_z3(int i) {
+  constexpr int v[Q3] = {0, 1, 2, 3, 4, 6, 5, 7, 8, 15, 16, 17, 18, 13, 14, 9, 10, 11, 12};
+  return v[i];
+}
+
+template <class R>
+__host__ __device__ __forceinline__ R w3(int i) {
+  return i == 0 ? R(1) / R(3) : (i <= 6 ? R(1) / R(18) : R(1) / R(36));
+}
+
+// ---------------- storage codecs ----------------
+struct CodecF32 {
+  using S = float;
+  using R = float;
+  static constexpr int prec = 0;
+  __device__ __forceinline__ static R load(const S* p) { return __ldg(p); }
+  __device__ __forceinline__ static R cvt(S v) { return v; }
+  __device__ __forceinline__ static S enc(R v) { return v; }
+};
+struct CodecF16 {
+  using S = __half;
+  using R = float;
+  static constexpr int prec = 1;
+  __device__ __forceinline__ static R cvt(S v) { return __half2float(v) * (1.0f / 32768.0f); }
+  __device__ __forceinline__ static R load(const S* p) { return cvt(__ldg(p)); }
+  __device__ __forceinline__ static S enc(R v) {
+    return __float2half_rn(fminf(fmaxf(v, -1.99f), 1.99f) * 32768.0f);
+  }
+};
+struct CodecBF16 {
+  using S = __nv_bfloat16;
+  using R = float;
+  static constexpr int prec = 2;
+  __device__ __forceinline__ static R cvt(S v) { return __bfloat162float(v); }
+  __device__ __forceinline__ static R load(const S* p) { return cvt(__ldg(p)); }
+  __device__ __forceinline__ static S enc(R v) { return __float2bfloat16_rn(v); }
+};
+struct CodecF64 {
+  using S = double;
+  using R = double;
+  static constexpr int prec = 3;
+  __device__ __forceinline__ static R load(const S* p) { return __ldg(p); }
+  __device__ __forceinline__ static R cvt(S v) { return v; }
+  __device__ __forceinline__ static S enc(R v) { return v; }
+};
+
+// Per-handle device state. step[] and uIn[] are double-buffered by parity: the step kernel of
+// parity p reads slot p and block 0 writes slot p^1 for the next step, so no kernel ever reads a
+// slot that the same kernel writes.
+struct DevState3 {
+  unsigned int step[2];
+  unsigned int sample;  // force samples written so far (the reference's histState)
+  unsigned int done;    // force blocks finished in the current sampled step
+  unsigned int status;  // bit 0: non-finite force sample, bit 1: non-finite macro value
+  unsigned int pad[3];
+  double uIn[2];
+};
+
+// Launch-invariant parameters of a step (kernel arguments). The x-dependent relaxation rate and
+// absorbing strength come from a per-x table that the host fills with the reference's arithmetic.
+template <class R>
+struct StepParams3 {
+  int W, H, D, N;
+  int nForceBlocks;
+  int rampKind;       // 0 none, 1 linear, 2 smoothstep
+  int rampEvery;
+  int pad;
+  double rampTarget;
+  double rampSteps;
+  R lambda;
+  R smagC2;
+};
+
+}  // namespace cells

@@ -1,0 +1,128 @@
+#include "device.h"
+
+#include <cstdlib>
+
+namespace cells {
+
+int64_t g_fake_live_buffers = 0;
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  if (e == cudaErrorMemoryAllocation) throw AllocError(std::string(what) + ": " + cudaGetErrorString(e));
+  throw Error(4 /*CELLS_E_CUDA*/, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void Device::open(int device_ordinal, int fail_alloc_at) {
+  ordinal = device_ordinal;
+  failAllocAt = fail_alloc_at;
+  if (device_ordinal == -2) {
+    fake = true;
+    return;
+  }
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    throw Error(4, std::string("no CUDA device available: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "0 devices"));
+  if (device_ordinal < 0 || device_ordinal >= n) throw Error(3, "device ordinal out of range");
+  check_cuda(cudaSetDevice(device_ordinal), "cudaSetDevice");
+  check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  check_cuda(cudaEventCreate(&ev0), "cudaEventCreate");
+  check_cuda(cudaEventCreate(&ev1), "cudaEventCreate");
+  check_cuda(cudaEventCreateWithFlags(&evRead, cudaEventDisableTiming), "cudaEventCreate");
+}
+
+void Device::close() {
+  if (fake) {
+    for (void* p : owned) {
+      std::free(p);
+      g_fake_live_buffers--;
+    }
+    owned.clear();
+    return;
+  }
+  if (stream) cudaStreamSynchronize(stream);
+  for (void* p : owned) cudaFree(p);
+  owned.clear();
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (evRead) cudaEventDestroy(evRead);
+  if (stream) cudaStreamDestroy(stream);
+  ev0 = ev1 = evRead = nullptr;
+  stream = nullptr;
+}
+
+void* Device::alloc(size_t bytes, const char* what) {
+  nAllocs++;
+  if (bytes == 0) bytes = 16;
+  if (fake) {
+    if (failAllocAt > 0 && nAllocs == failAllocAt)
+      throw AllocError(std::string("fake out-of-memory allocating ") + what);
+    void* p = std::calloc(1, bytes);
+    if (!p) throw AllocError(std::string("host out of memory allocating ") + what);
+    owned.push_back(p);
+    g_fake_live_buffers++;
+    return p;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // clear the sticky-free allocation error
+    throw AllocError(std::string(what) + " (" + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e));
+  }
+  owned.push_back(p);
+  return p;
+}
+
+void Device::h2d(void* d, const void* h, size_t bytes) {
+  if (fake) {
+    std::memcpy(d, h, bytes);
+    return;
+  }
+  check_cuda(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync H2D");
+}
+
+void Device::d2h(void* h, const void* d, size_t bytes) {
+  if (fake) {
+    std::memcpy(h, d, bytes);
+    return;
+  }
+  check_cuda(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync D2H");
+}
+
+void Device::memset0(void* d, size_t bytes) {
+  if (fake) {
+    std::memset(d, 0, bytes);
+    return;
+  }
+  check_cuda(cudaMemsetAsync(d, 0, bytes, stream), "cudaMemsetAsync");
+}
+
+void Device::sync() {
+  if (fake) return;
+  check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+}
+
+void* Device::host_pinned(size_t bytes) {
+  if (fake) return std::calloc(1, bytes);
+  void* p = nullptr;
+  check_cuda(cudaMallocHost(&p, bytes), "cudaMallocHost");
+  return p;
+}
+
+void Device::free_host_pinned(void* p) {
+  if (!p) return;
+  if (fake) {
+    std::free(p);
+    return;
+  }
+  cudaFreeHost(p);
+}
+
+size_t Device::free_bytes() {
+  if (fake) return (size_t)1 << 40;
+  size_t fr = 0, tot = 0;
+  check_cuda(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+  return fr;
+}
+
+}  // namespace cells

@@ -1,0 +1,55 @@
+// Device memory, stream and error plumbing shared by the 2D and 3D solvers.
+//
+// A Device is either a CUDA device (one non-blocking stream per solver handle) or the fake device
+// (CELLS_FAKE_DEVICE): host memory, no kernels, used only by the host-logic tests.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace cells {
+
+struct Error : std::runtime_error {
+  int status;
+  Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+// Thrown by Device::alloc; the solver turns it into "Solver3D allocation failed: <what>".
+struct AllocError : std::runtime_error {
+  explicit AllocError(const std::string& m) : std::runtime_error(m) {}
+};
+
+void check_cuda(cudaError_t e, const char* what);
+
+struct Device {
+  bool fake = false;
+  int ordinal = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evRead = nullptr;
+  int failAllocAt = 0;  // fake device only: the n-th allocation (1-based) fails
+  int nAllocs = 0;
+  std::vector<void*> owned;
+  int64_t launches = 0;
+
+  void open(int device_ordinal, int fail_alloc_at);
+  void close();
+  void* alloc(size_t bytes, const char* what);
+  void h2d(void* d, const void* h, size_t bytes);
+  void d2h(void* h, const void* d, size_t bytes);
+  void memset0(void* d, size_t bytes);
+  void sync();
+  void* host_pinned(size_t bytes);
+  void free_host_pinned(void* p);
+  size_t free_bytes();
+};
+
+// Number of live fake-device buffers in the process (host-logic tests check that a failed create
+// frees everything).
+extern int64_t g_fake_live_buffers;
+
+}  // namespace cells

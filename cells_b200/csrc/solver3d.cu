@@ -1,0 +1,738 @@
+// Solver3D host state and the 3D half of the C ABI (include/cells.h).
+//
+// Mirrors class Solver3D, src/solver3d.ts:42-320: buffers, parameter derivation (writeParams
+// :197-208), setSdf/rebuildFlags (:211-228), initField (:231-242), resetForces (:244-249),
+// encodeSteps (:252-267), run (:276-288), readMacro (:290-292) and readForces with its ring window
+// and generation check (:295-315). Everything is enqueued on the handle's own CUDA stream.
+#include <cmath>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cells.h"
+#include "device.h"
+#include "kernels3d.h"
+
+namespace cells {
+thread_local std::string g_create_error;
+}
+
+using namespace cells;
+
+struct Cells3D {
+  Device dev;
+  Cells3DConfig cfg{};
+  int W = 0, H = 0, D = 0;
+  long long N = 0;
+  int prec = 0;
+  size_t bpp = 4;  // bytes per stored population
+  int bx = 32, by = 1;
+  int gx = 1, gy = 1, nBlocks = 1;
+
+  void* f[2] = {nullptr, nullptr};
+  uint32_t* flags = nullptr;
+  float* sdf = nullptr;
+  uint8_t* rowBody = nullptr;
+  void* xTab = nullptr;
+  int* blockSlot = nullptr;
+  double4* partials = nullptr;
+  double4* history = nullptr;
+  DevState3* st = nullptr;
+  float4* macro = nullptr;
+  double* massPartials = nullptr;
+  double* massOut = nullptr;
+  int nMassPartials = 0;
+
+  // host bookkeeping (src/solver3d.ts:48-54)
+  int64_t step = 0;
+  int parity = 0;
+  uint64_t forceSamplesRead = 0;
+  std::deque<uint32_t> forceSteps;
+  uint64_t forceGeneration = 0;
+  int nForceBlocks = 1;
+
+  // inlet
+  double uIn = 0.0;
+  int rampKind = 0;
+  double rampTarget = 0.0;
+  int64_t rampSteps = 1, rampEvery = 1;
+
+  // staging for readForces
+  double4* stageHist = nullptr;  // pinned, HISTORY_LEN entries
+  unsigned* stageState = nullptr;
+  bool readPending = false;
+  uint64_t readGeneration = 0;
+  uint64_t readFirst = 0, readWritten = 0;
+
+  double fakeForce[3] = {0, 0, 0};
+  std::string lastError;
+
+  double lambda_value() const {
+    if (std::isnan(cfg.lambda)) return std::fmin(3.0 / 16.0, 50.0 * (cfg.tau - 0.5) * (cfg.tau - 0.5));
+    return cfg.lambda;
+  }
+  double sponge_start() const { return cfg.sponge_fraction > 0 ? (W - 1) * (1 - cfg.sponge_fraction) : 1e9; }
+  double tau_sponge() const { return std::fmax(cfg.sponge_tau, cfg.tau); }
+  double ramp_speed(int64_t s) const {
+    const int64_t q = (s / rampEvery) * rampEvery;
+    const double t = std::fmin(1.0, (double)q / (double)rampSteps);
+    return rampKind == 1 ? rampTarget * t : rampTarget * (t * t * (3.0 - 2.0 * t));
+  }
+  double current_uin() const { return rampKind ? ramp_speed(step) : uIn; }
+
+  void choose_launch();
+  void upload_xtab();
+  void rebuild_flags();
+  void build_block_slots(const std::vector<uint8_t>& rows);
+  void launch_steps(int64_t n);
+  void write_state(int which);
+  void free_all();
+};
+
+// ---------------- helpers ----------------
+
+template <class R>
+static void fill_xtab(std::vector<R>& t, int W, double tau, double spongeStart, double tauSponge, double absorb) {
+  // The reference computes these per cell in f32 (src/shaders/step3d.ts:213-219); the same f32
+  // operations in the same order give the same values here (no FMA contraction on the host).
+  const R tauR = (R)tau, ssR = (R)spongeStart, tsR = (R)tauSponge, abR = (R)absorb;
+  const R e1 = (R)(W - 1);
+  t.resize(2 * (size_t)W);
+  for (int x = 0; x < W; x++) {
+    R omegaBase = R(1) / tauR;
+    R sOut = R(0);
+    if (ssR < e1) {
+      R tt = (R(x) - ssR) / (e1 - ssR);
+      tt = std::fmin(std::fmax(tt, R(0)), R(1));
+      sOut = tt * tt * (R(3) - R(2) * tt);
+      const R mix = tauR * (R(1) - sOut) + tsR * sOut;
+      omegaBase = R(1) / mix;
+    }
+    t[2 * x] = omegaBase;
+    t[2 * x + 1] = abR * sOut * sOut;
+  }
+}
+
+void Cells3D::choose_launch() {
+  int threads = cfg.workgroup_size > 0 ? cfg.workgroup_size : 256;
+  if (threads > 256) threads = 256;
+  if (threads < 32) threads = 32;
+  threads &= ~31;
+  int best = -1;
+  long long bestWaste = -1;
+  for (int c = 256; c >= 32; c >>= 1) {
+    if (c > threads) continue;
+    const long long waste = (long long)((W + c - 1) / c) * c - W;
+    if (best < 0 || waste < bestWaste) {
+      best = c;
+      bestWaste = waste;
+    }
+  }
+  bx = best;
+  by = threads / bx;
+  while (by > 1 && (H % by) != 0 && ((H + by - 1) / by) * by - H > H / 8) by >>= 1;
+  if (by < 1) by = 1;
+  gx = (W + bx - 1) / bx;
+  gy = (H + by - 1) / by;
+  nBlocks = gx * gy * D;
+}
+
+void Cells3D::upload_xtab() {
+  if (prec == 3) {
+    std::vector<double> t;
+    fill_xtab<double>(t, W, cfg.tau, sponge_start(), tau_sponge(), cfg.absorb);
+    dev.h2d(xTab, t.data(), t.size() * sizeof(double));
+  } else {
+    std::vector<float> t;
+    fill_xtab<float>(t, W, cfg.tau, sponge_start(), tau_sponge(), cfg.absorb);
+    dev.h2d(xTab, t.data(), t.size() * sizeof(float));
+  }
+  if (!dev.fake) dev.sync();  // the host vectors die here
+}
+
+void Cells3D::write_state(int which) {
+  // which: 1 step counters, 2 inlet speeds, 4 clear samples, 8 clear status
+  if (dev.fake) {
+    if (which & 1) st->step[0] = st->step[1] = (unsigned)step;
+    if (which & 2) st->uIn[0] = st->uIn[1] = current_uin();
+    if (which & 4) st->sample = st->done = 0;
+    if (which & 8) st->status = 0;
+    return;
+  }
+  const double u = current_uin();
+  check_cuda(launch_set_state3(st, which, (unsigned)step, u, u, dev.stream), "set_state kernel");
+  dev.launches++;
+}
+
+void Cells3D::build_block_slots(const std::vector<uint8_t>& rows) {
+  std::vector<int> slots((size_t)nBlocks, -1);
+  int k = 0;
+  for (int z = 0; z < D; z++)
+    for (int byi = 0; byi < gy; byi++) {
+      bool body = false;
+      for (int y = byi * by; y < std::min(H, (byi + 1) * by); y++) body = body || rows[(size_t)y + (size_t)H * z];
+      for (int bxi = 0; bxi < gx; bxi++) {
+        const size_t b = (size_t)bxi + (size_t)gx * ((size_t)byi + (size_t)gy * z);
+        if (body || b == 0) slots[b] = k++;
+      }
+    }
+  nForceBlocks = k;
+  dev.h2d(blockSlot, slots.data(), slots.size() * sizeof(int));
+  if (!dev.fake) dev.sync();
+}
+
+// rebuildFlags, src/solver3d.ts:216-228: a macro pass on the latest populations (the refill reads
+// it), then the flags pass, then the body-row map that picks the force blocks.
+void Cells3D::rebuild_flags() {
+  std::vector<uint8_t> rows((size_t)H * D, 0);
+  if (!dev.fake) {
+    AuxLaunch3 a{W, H, D, (int)N, uIn};
+    a.uIn = current_uin();
+    check_cuda(launch_macro3(prec, a, f[parity], flags, macro, st, dev.stream), "macro kernel");
+    dev.memset0(rowBody, (size_t)H * D);
+    check_cuda(launch_flags3(prec, a, sdf, flags, rowBody, f[0], f[1], macro, dev.stream), "flags kernel");
+    dev.launches += 2;
+    dev.d2h(rows.data(), rowBody, rows.size());
+    dev.sync();
+  }
+  build_block_slots(rows);
+}
+
+void Cells3D::launch_steps(int64_t n) {
+  const int every = cfg.force_every;
+  for (int64_t k = 0; k < n; k++) {
+    const bool sample = every > 0 && ((step + 1) % every) == 0;
+    if (dev.fake) {
+      if (sample) {
+        const unsigned s = st->sample;
+        history[s % HISTORY_LEN] = make_double4(fakeForce[0], fakeForce[1], fakeForce[2], 0.0);
+        st->sample = s + 1;
+      }
+    } else {
+      StepLaunch3 a;
+      a.src = f[parity];
+      a.dst = f[parity ^ 1];
+      a.flags = flags;
+      a.sdf = sdf;
+      a.rowBody = rowBody;
+      a.xTab = xTab;
+      a.blockSlot = blockSlot;
+      a.partials = partials;
+      a.history = history;
+      a.st = st;
+      a.W = W;
+      a.H = H;
+      a.D = D;
+      a.N = (int)N;
+      a.bx = bx;
+      a.by = by;
+      a.nForceBlocks = nForceBlocks;
+      a.rampKind = rampKind;
+      a.rampEvery = (int)rampEvery;
+      a.rampTarget = rampTarget;
+      a.rampSteps = (double)rampSteps;
+      a.lambda = lambda_value();
+      a.smagC2 = cfg.smagorinsky * cfg.smagorinsky;
+      a.par = parity;
+      a.sample = sample ? 1 : 0;
+      check_cuda(cfg.arithmetic == CELLS_ARITH_EXACT ? exact::launch_step3(prec, a, dev.stream)
+                                                     : fast::launch_step3(prec, a, dev.stream),
+                 "step kernel");
+      dev.launches++;
+    }
+    parity ^= 1;
+    step++;
+    if (sample) forceSteps.push_back((uint32_t)step);
+  }
+}
+
+void Cells3D::free_all() {
+  if (stageHist) dev.free_host_pinned(stageHist);
+  if (stageState) dev.free_host_pinned(stageState);
+  stageHist = nullptr;
+  stageState = nullptr;
+  dev.close();
+}
+
+// ---------------- C ABI ----------------
+
+#define CELLS_TRY(h)                                   \
+  try {
+#define CELLS_CATCH(h)                                 \
+  }                                                    \
+  catch (const AllocError& e) {                        \
+    (h)->lastError = std::string("Solver3D allocation failed: ") + e.what(); \
+    return CELLS_E_ALLOC;                              \
+  }                                                    \
+  catch (const Error& e) {                             \
+    (h)->lastError = e.what();                         \
+    return e.status;                                   \
+  }                                                    \
+  catch (const std::exception& e) {                    \
+    (h)->lastError = e.what();                         \
+    return CELLS_E_INVALID;                            \
+  }                                                    \
+  return CELLS_OK;
+
+extern "C" {
+
+void cells3d_config_default(Cells3DConfig* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->precision = CELLS_FP32;
+  c->tau = 0.6;
+  c->lambda = NAN;
+  c->smagorinsky = 0.0;
+  c->u_in = 0.0;
+  c->sponge_fraction = 0.0;
+  c->sponge_tau = 1.0;
+  c->absorb = 0.0;
+  c->workgroup_size = 0;
+  c->force_every = 1;
+  c->device = 0;
+}
+
+const char* cells_last_error(const void* h) {
+  if (!h) return g_create_error.c_str();
+  return ((const Cells3D*)h)->lastError.c_str();
+}
+
+int cells3d_create(const Cells3DConfig* cfg, Cells3D** out) {
+  if (!out) return CELLS_E_INVALID;
+  *out = nullptr;
+  g_create_error.clear();
+  if (!cfg) {
+    g_create_error = "config is NULL";
+    return CELLS_E_INVALID;
+  }
+  if (cfg->width < 3 || cfg->height < 1 || cfg->depth < 1) {
+    g_create_error = "grid must be at least 3 x 1 x 1";
+    return CELLS_E_INVALID;
+  }
+  if (cfg->precision < 0 || cfg->precision > 3) {
+    g_create_error = "precision " + std::to_string(cfg->precision) + " is not available on this device";
+    return CELLS_E_PRECISION_UNSUPPORTED;
+  }
+  if (!(cfg->tau > 0.5)) {
+    g_create_error = "tau must be above 1/2";
+    return CELLS_E_INVALID;
+  }
+  const long long N = (long long)cfg->width * cfg->height * cfg->depth;
+  if (N > 0x7fffffffLL) {
+    g_create_error = "grid has more than 2^31 cells";
+    return CELLS_E_INVALID;
+  }
+  Cells3D* h = new Cells3D();
+  h->cfg = *cfg;
+  h->W = cfg->width;
+  h->H = cfg->height;
+  h->D = cfg->depth;
+  h->N = N;
+  h->prec = cfg->precision;
+  h->bpp = h->prec == 0 ? 4 : (h->prec == 3 ? 8 : 2);
+  h->uIn = cfg->u_in;
+  try {
+    h->dev.open(cfg->device, cfg->fake_fail_alloc);
+    const unsigned long long fBytes = 19ull * h->bpp * (unsigned long long)N;
+    // fitsLimits (src/shaders/common3d.ts:67-70): checked before anything is allocated
+    if (cfg->max_buffer_bytes > 0 && fBytes > cfg->max_buffer_bytes) {
+      throw AllocError("one distribution buffer needs " + std::to_string(fBytes) + " bytes; this device allows " +
+                       std::to_string(cfg->max_buffer_bytes) + " per buffer");
+    }
+    h->choose_launch();
+    const unsigned long long total = 2 * fBytes + (unsigned long long)N * (4 + 4 + 16) + (1u << 22);
+    const size_t freeB = h->dev.free_bytes();
+    if (total > freeB) {
+      throw AllocError("the solver needs " + std::to_string(total) + " bytes; this device has " +
+                       std::to_string(freeB) + " bytes free");
+    }
+    h->f[0] = h->dev.alloc(fBytes, "distribution buffer A");
+    h->f[1] = h->dev.alloc(fBytes, "distribution buffer B");
+    h->flags = (uint32_t*)h->dev.alloc((size_t)N * 4, "flags");
+    h->sdf = (float*)h->dev.alloc((size_t)N * 4, "sdf");
+    h->macro = (float4*)h->dev.alloc((size_t)N * 16, "macro");
+    h->rowBody = (uint8_t*)h->dev.alloc((size_t)h->H * h->D, "row map");
+    h->xTab = h->dev.alloc((size_t)h->W * 2 * (h->prec == 3 ? 8 : 4), "x table");
+    h->blockSlot = (int*)h->dev.alloc((size_t)h->nBlocks * 4, "block slots");
+    h->partials = (double4*)h->dev.alloc((size_t)h->nBlocks * sizeof(double4), "force partials");
+    h->history = (double4*)h->dev.alloc((size_t)HISTORY_LEN * sizeof(double4), "force history");
+    h->st = (DevState3*)h->dev.alloc(sizeof(DevState3), "state");
+    h->nMassPartials = 4 * 148;
+    h->massPartials = (double*)h->dev.alloc((size_t)h->nMassPartials * 8, "mass partials");
+    h->massOut = (double*)h->dev.alloc(8, "mass result");
+    h->stageHist = (double4*)h->dev.host_pinned((size_t)HISTORY_LEN * sizeof(double4));
+    h->stageState = (unsigned*)h->dev.host_pinned(64);
+    // zero state, fill the SDF with FAR = 1e6 (src/solver3d.ts:142)
+    h->dev.memset0(h->st, sizeof(DevState3));
+    h->dev.memset0(h->f[0], fBytes);
+    h->dev.memset0(h->f[1], fBytes);
+    h->dev.memset0(h->flags, (size_t)N * 4);
+    {
+      std::vector<float> far((size_t)N, 1e6f);
+      h->dev.h2d(h->sdf, far.data(), far.size() * 4);
+      h->dev.sync();
+    }
+    h->upload_xtab();
+    h->write_state(1 | 2 | 4 | 8);
+    h->rebuild_flags();
+  } catch (const AllocError& e) {
+    g_create_error = std::string("Solver3D allocation failed: ") + e.what();
+    h->free_all();
+    delete h;
+    return CELLS_E_ALLOC;
+  } catch (const Error& e) {
+    g_create_error = e.what();
+    h->free_all();
+    delete h;
+    return e.status;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    h->free_all();
+    delete h;
+    return CELLS_E_INVALID;
+  }
+  *out = h;
+  return CELLS_OK;
+}
+
+void cells3d_destroy(Cells3D* h) {
+  if (!h) return;
+  h->free_all();
+  delete h;
+}
+
+int cells3d_set_tau(Cells3D* h, double tau) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  if (!(tau > 0.5)) throw Error(CELLS_E_INVALID, "tau must be above 1/2");
+  h->cfg.tau = tau;
+  h->upload_xtab();
+  CELLS_CATCH(h)
+}
+
+int cells3d_set_smagorinsky(Cells3D* h, double cs) {
+  if (!h) return CELLS_E_INVALID;
+  h->cfg.smagorinsky = cs;
+  return CELLS_OK;
+}
+
+int cells3d_set_lambda(Cells3D* h, double lambda) {
+  if (!h) return CELLS_E_INVALID;
+  h->cfg.lambda = lambda;
+  return CELLS_OK;
+}
+
+int cells3d_set_inlet(Cells3D* h, double u) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  h->uIn = u;
+  h->cfg.u_in = u;
+  h->rampKind = 0;
+  h->write_state(2);
+  CELLS_CATCH(h)
+}
+
+int cells3d_set_inlet_ramp(Cells3D* h, int kind, double target, int64_t ramp_steps, int64_t update_every) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  if (kind < 0 || kind > 2) throw Error(CELLS_E_INVALID, "unknown ramp kind");
+  if (kind != 0 && (ramp_steps <= 0 || update_every <= 0))
+    throw Error(CELLS_E_INVALID, "ramp_steps and update_every must be positive");
+  h->rampKind = kind;
+  h->rampTarget = target;
+  h->rampSteps = ramp_steps > 0 ? ramp_steps : 1;
+  h->rampEvery = update_every > 0 ? update_every : 1;
+  if (kind == 0) h->uIn = target;
+  h->write_state(2);
+  CELLS_CATCH(h)
+}
+
+int cells3d_set_sdf(Cells3D* h, const float* sdf, size_t n) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  if (!sdf || n != (size_t)h->N) throw Error(CELLS_E_INVALID, "set_sdf needs W*H*D floats");
+  h->dev.h2d(h->sdf, sdf, n * 4);
+  h->dev.sync();
+  h->rebuild_flags();
+  CELLS_CATCH(h)
+}
+
+int cells3d_init_field(Cells3D* h, const float* macro4n) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  h->step = 0;
+  h->parity = 0;
+  if (!h->dev.fake) {
+    if (macro4n) {
+      h->dev.h2d(h->macro, macro4n, (size_t)h->N * 16);
+    }
+    AuxLaunch3 a{h->W, h->H, h->D, (int)h->N, h->current_uin()};
+    check_cuda(launch_init3(h->prec, a, h->f[0], h->f[1], h->flags, macro4n ? h->macro : nullptr, h->dev.stream),
+               "init kernel");
+    h->dev.launches++;
+    if (macro4n) h->dev.sync();
+  }
+  h->write_state(1 | 2);
+  // resetForces (src/solver3d.ts:244-249)
+  h->write_state(4);
+  h->forceSamplesRead = 0;
+  h->forceSteps.clear();
+  h->forceGeneration++;
+  CELLS_CATCH(h)
+}
+
+int cells3d_reset_forces(Cells3D* h) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  h->write_state(4);
+  h->forceSamplesRead = 0;
+  h->forceSteps.clear();
+  h->forceGeneration++;
+  CELLS_CATCH(h)
+}
+
+int cells3d_step(Cells3D* h, int64_t n) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  if (n < 0) throw Error(CELLS_E_INVALID, "negative step count");
+  h->launch_steps(n);
+  CELLS_CATCH(h)
+}
+
+int cells3d_update_macro(Cells3D* h) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  if (!h->dev.fake) {
+    AuxLaunch3 a{h->W, h->H, h->D, (int)h->N, h->current_uin()};
+    check_cuda(launch_macro3(h->prec, a, h->f[h->parity], h->flags, h->macro, h->st, h->dev.stream), "macro kernel");
+    h->dev.launches++;
+  }
+  CELLS_CATCH(h)
+}
+
+int cells3d_run(Cells3D* h, int64_t n, int64_t chunk) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  if (n < 0) throw Error(CELLS_E_INVALID, "negative step count");
+  if (chunk <= 0) chunk = 500;
+  for (int64_t done = 0; done < n;) {
+    const int64_t k = std::min(chunk, n - done);
+    h->launch_steps(k);
+    done += k;
+  }
+  int rc = cells3d_update_macro(h);
+  if (rc != CELLS_OK) return rc;
+  h->dev.sync();
+  CELLS_CATCH(h)
+}
+
+int cells3d_synchronize(Cells3D* h) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  h->dev.sync();
+  CELLS_CATCH(h)
+}
+
+int cells3d_read_macro(Cells3D* h, float* out4n) {
+  if (!h || !out4n) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  h->dev.d2h(out4n, h->macro, (size_t)h->N * 16);
+  h->dev.sync();
+  CELLS_CATCH(h)
+}
+
+int cells3d_read_forces_begin(Cells3D* h) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  h->readPending = false;
+  if (h->forceSteps.empty()) return CELLS_OK;
+  const uint64_t written = h->forceSamplesRead + h->forceSteps.size();
+  const uint64_t first = std::max<uint64_t>(h->forceSamplesRead, written > (uint64_t)HISTORY_LEN ? written - HISTORY_LEN : 0);
+  // copy ring entries [first, written) in order into the staging buffer (at most two runs)
+  uint64_t k = first;
+  size_t outPos = 0;
+  while (k < written) {
+    const size_t r = (size_t)(k % HISTORY_LEN);
+    const size_t run = (size_t)std::min<uint64_t>(written - k, (uint64_t)(HISTORY_LEN - r));
+    h->dev.d2h(h->stageHist + outPos, h->history + r, run * sizeof(double4));
+    outPos += run;
+    k += run;
+  }
+  h->dev.d2h(h->stageState, &h->st->sample, sizeof(unsigned));
+  if (!h->dev.fake) check_cuda(cudaEventRecord(h->dev.evRead, h->dev.stream), "cudaEventRecord");
+  h->readPending = true;
+  h->readGeneration = h->forceGeneration;
+  h->readFirst = first;
+  h->readWritten = written;
+  CELLS_CATCH(h)
+}
+
+int cells3d_read_forces_end(Cells3D* h, CellsForceSample* out, size_t cap, size_t* n_out) {
+  if (!h || !n_out) return CELLS_E_INVALID;
+  *n_out = 0;
+  CELLS_TRY(h)
+  if (!h->readPending) return CELLS_OK;
+  if (!h->dev.fake) check_cuda(cudaEventSynchronize(h->dev.evRead), "cudaEventSynchronize");
+  // a reset while the copy was in flight makes these samples stale
+  if (h->readGeneration != h->forceGeneration) {
+    h->readPending = false;
+    return CELLS_OK;
+  }
+  const uint64_t n = h->readWritten - h->readFirst;
+  if (n > cap) throw Error(CELLS_E_INVALID, "read_forces needs room for " + std::to_string(n) + " samples");
+  if ((uint64_t)*h->stageState != (h->readWritten & 0xffffffffull))
+    throw Error(CELLS_E_INVALID, "force ring counter " + std::to_string(*h->stageState) + " does not match the " +
+                                     std::to_string(h->readWritten) + " samples enqueued");
+  for (uint64_t k = 0; k < n; k++) {
+    const double4 v = h->stageHist[k];
+    out[k].step = h->forceSteps[(size_t)(h->readFirst + k - h->forceSamplesRead)];
+    out[k].reserved = 0;
+    out[k].fx = v.x;
+    out[k].fy = v.y;
+    out[k].fz = v.z;
+  }
+  const size_t consumed = (size_t)(h->readWritten - h->forceSamplesRead);
+  h->forceSteps.erase(h->forceSteps.begin(), h->forceSteps.begin() + consumed);
+  h->forceSamplesRead = h->readWritten;
+  h->readPending = false;
+  *n_out = (size_t)n;
+  CELLS_CATCH(h)
+}
+
+int cells3d_read_forces(Cells3D* h, CellsForceSample* out, size_t cap, size_t* n_out) {
+  int rc = cells3d_read_forces_begin(h);
+  if (rc != CELLS_OK) return rc;
+  return cells3d_read_forces_end(h, out, cap, n_out);
+}
+
+int cells3d_read_status(Cells3D* h, uint32_t* status) {
+  if (!h || !status) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  h->dev.d2h(h->stageState + 1, &h->st->status, sizeof(unsigned));
+  h->dev.sync();
+  *status = h->stageState[1];
+  CELLS_CATCH(h)
+}
+
+int cells3d_get_info(Cells3D* h, Cells3DInfo* info) {
+  if (!h || !info) return CELLS_E_INVALID;
+  info->W = h->W;
+  info->H = h->H;
+  info->D = h->D;
+  info->precision = h->prec;
+  info->N = h->N;
+  info->step = h->step;
+  info->block_x = h->bx;
+  info->block_y = h->by;
+  info->force_every = h->cfg.force_every;
+  info->n_force_blocks = h->nForceBlocks;
+  return CELLS_OK;
+}
+
+int cells3d_read_params(Cells3D* h, void* out64) {
+  if (!h || !out64) return CELLS_E_INVALID;
+  uint32_t u[16] = {0};
+  float* f = (float*)u;
+  u[0] = (uint32_t)h->W;
+  u[1] = (uint32_t)h->H;
+  u[2] = (uint32_t)h->D;
+  u[3] = (uint32_t)h->N;
+  u[4] = (uint32_t)h->gx;
+  f[8] = (float)h->cfg.tau;
+  f[9] = (float)h->lambda_value();
+  f[10] = (float)(h->cfg.smagorinsky * h->cfg.smagorinsky);
+  f[11] = (float)h->current_uin();
+  f[12] = (float)h->sponge_start();
+  f[13] = (float)h->tau_sponge();
+  f[14] = (float)h->cfg.absorb;
+  std::memcpy(out64, u, 64);
+  return CELLS_OK;
+}
+
+int cells3d_mass(Cells3D* h, double* out) {
+  if (!h || !out) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  if (h->dev.fake) throw Error(CELLS_E_INVALID, "mass needs a CUDA device");
+  AuxLaunch3 a{h->W, h->H, h->D, (int)h->N, h->current_uin()};
+  check_cuda(launch_mass3(h->prec, a, h->f[h->parity], h->flags, h->massPartials, h->nMassPartials, h->massOut,
+                          h->dev.stream),
+             "mass kernel");
+  h->dev.launches += 2;
+  double v = 0;
+  h->dev.d2h(h->stageState + 2, h->massOut, 8);  // 8-byte aligned slot in the pinned block
+  h->dev.sync();
+  std::memcpy(&v, h->stageState + 2, 8);
+  *out = v;
+  CELLS_CATCH(h)
+}
+
+int cells3d_read_populations(Cells3D* h, void* out, size_t bytes) {
+  if (!h || !out) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  const size_t need = 19ull * h->bpp * (size_t)h->N;
+  if (bytes != need) throw Error(CELLS_E_INVALID, "read_populations needs " + std::to_string(need) + " bytes");
+  h->dev.d2h(out, h->f[h->parity], need);
+  h->dev.sync();
+  CELLS_CATCH(h)
+}
+
+int cells3d_write_populations(Cells3D* h, const void* in, size_t bytes) {
+  if (!h || !in) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  const size_t need = 19ull * h->bpp * (size_t)h->N;
+  if (bytes != need) throw Error(CELLS_E_INVALID, "write_populations needs " + std::to_string(need) + " bytes");
+  h->dev.h2d(h->f[h->parity], in, need);
+  h->dev.sync();
+  CELLS_CATCH(h)
+}
+
+int cells3d_read_flags(Cells3D* h, uint32_t* out, size_t n) {
+  if (!h || !out) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  if (n != (size_t)h->N) throw Error(CELLS_E_INVALID, "read_flags needs N entries");
+  h->dev.d2h(out, h->flags, n * 4);
+  h->dev.sync();
+  CELLS_CATCH(h)
+}
+
+int cells3d_timer_start(Cells3D* h) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  if (!h->dev.fake) check_cuda(cudaEventRecord(h->dev.ev0, h->dev.stream), "cudaEventRecord");
+  CELLS_CATCH(h)
+}
+
+int cells3d_timer_stop(Cells3D* h, float* ms) {
+  if (!h || !ms) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  *ms = 0.f;
+  if (!h->dev.fake) {
+    check_cuda(cudaEventRecord(h->dev.ev1, h->dev.stream), "cudaEventRecord");
+    check_cuda(cudaEventSynchronize(h->dev.ev1), "cudaEventSynchronize");
+    check_cuda(cudaEventElapsedTime(ms, h->dev.ev0, h->dev.ev1), "cudaEventElapsedTime");
+  }
+  CELLS_CATCH(h)
+}
+
+int cells3d_launch_count(Cells3D* h, int64_t* count) {
+  if (!h || !count) return CELLS_E_INVALID;
+  *count = h->dev.launches;
+  return CELLS_OK;
+}
+
+int cells3d_fake_set_force(Cells3D* h, double fx, double fy, double fz) {
+  if (!h) return CELLS_E_INVALID;
+  if (!h->dev.fake) {
+    h->lastError = "fake_set_force is only for CELLS_FAKE_DEVICE handles";
+    return CELLS_E_INVALID;
+  }
+  h->fakeForce[0] = fx;
+  h->fakeForce[1] = fy;
+  h->fakeForce[2] = fz;
+  return CELLS_OK;
+}
+
+int64_t cells_fake_live_buffers(void) { return g_fake_live_buffers; }
+
+}  // extern "C"

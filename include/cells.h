@@ -1,0 +1,194 @@
+/*
+ * cells.h — C ABI of the B200 lattice Boltzmann wind-tunnel step engine (libcells.so).
+ *
+ * This is the drop-in boundary for the step API of slowernet/cells:
+ *   class Solver3D   src/solver3d.ts:42-320   (D3Q19, FP32 / FP16 storage; BF16 and FP64 added here)
+ *   class Solver     src/solver.ts:50-340     (D2Q9)
+ * A Node-API addon (or ctypes, or any FFI) binds these functions one to one; each handle owns one
+ * CUDA stream, and every call on a handle is ordered on that stream. Calls on one handle are not
+ * thread-safe; different handles are independent.
+ *
+ * Conventions
+ *   - Every function returns a cells_status; CELLS_OK is 0. cells_last_error(handle) gives the
+ *     message of the last failure on that handle (or of the last failed create when handle is NULL).
+ *   - Allocation failures use CELLS_E_ALLOC and a message that begins "Solver3D allocation failed: "
+ *     (or "Solver allocation failed: " in 2D), the prefix the reference's callers test for
+ *     (src/solver3d.ts:84-95, src/app3d.ts:180-190). A failed create frees everything it allocated.
+ *   - Distributions are stored shifted (f_i - w_i), structure-of-arrays f[i*N + cell] with
+ *     cell = x + W*(y + H*z), as in the reference (src/shaders/common3d.ts:34).
+ */
+#ifndef CELLS_H
+#define CELLS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CELLS_OK = 0,
+  CELLS_E_ALLOC = 1,                 /* "Solver3D allocation failed: ..." */
+  CELLS_E_PRECISION_UNSUPPORTED = 2, /* reference: 'shader-f16 is not available on this device' */
+  CELLS_E_INVALID = 3,               /* bad argument or call order */
+  CELLS_E_CUDA = 4,                  /* a CUDA runtime error; message has the CUDA error string */
+  CELLS_E_DIVERGED = 5,              /* a non-finite force or macro value was seen on the device */
+  CELLS_E_TIMEOUT = 6                /* a bounded device-side wait ran out */
+} cells_status;
+
+/* Storage precision of the distributions. Arithmetic is f32 except for CELLS_FP64 (f64).
+ * reference: Precision = 'fp16' | 'fp32' (src/shaders/common3d.ts:4). */
+typedef enum {
+  CELLS_FP32 = 0,
+  CELLS_FP16 = 1, /* f16 scaled by 2^15, clamped to +-1.99 before the store (src/shaders/common3d.ts:52-63) */
+  CELLS_BF16 = 2, /* bf16, unscaled, round to nearest even (not in the reference) */
+  CELLS_FP64 = 3  /* f64 storage and arithmetic: the GPU oracle run (not in the reference) */
+} cells_precision;
+
+/* Device ordinal that selects the fake device: buffers live in host memory and kernels are not
+ * run. It exists only to test the host-side logic (parameter packing, force-ring bookkeeping,
+ * error conventions) without a GPU, as the reference's fakeDevice() does in src/solver3d.test.ts:13-69. */
+#define CELLS_FAKE_DEVICE (-2)
+
+/* Step-kernel arithmetic. FAST lets the compiler fuse multiply-adds (the tuned default). EXACT
+ * rounds every operation as written (no contraction), which reproduces a non-FMA CPU evaluation of
+ * the reference formulas bit for bit; it is slower only in arithmetic-bound configurations. */
+#define CELLS_ARITH_FAST 0
+#define CELLS_ARITH_EXACT 1
+
+/* Inlet ramp kinds for cells3d_set_inlet_ramp (the reference ramps on the host: src/cases.ts:52-53). */
+typedef enum { CELLS_RAMP_NONE = 0, CELLS_RAMP_LINEAR = 1, CELLS_RAMP_SMOOTHSTEP = 2 } cells_ramp_kind;
+
+/* Solver3DConfig, src/solver3d.ts:11-31. Call cells3d_config_default() first: it fills the
+ * reference defaults (src/solver3d.ts:110-119); then set the fields you need. */
+typedef struct {
+  int32_t width, height, depth;
+  int32_t precision;        /* cells_precision */
+  double tau;
+  double lambda;            /* fixed TRT Lambda; NaN (default) follows trtLambda3(tau) */
+  double smagorinsky;       /* C_s; 0 disables the subgrid model */
+  double u_in;              /* inflow speed, already ramped by the caller */
+  double sponge_fraction;   /* fraction of the length, ending at the outlet, where tau rises */
+  double sponge_tau;
+  double absorb;            /* peak rate of the outlet absorbing layer; 0 disables it */
+  int32_t workgroup_size;   /* threads per block; 0 picks the tuned default */
+  int32_t force_every;      /* sample the obstacle force every n steps; 0 disables sampling */
+  int32_t device;           /* CUDA device ordinal, or CELLS_FAKE_DEVICE */
+  int32_t fake_fail_alloc;  /* fake device only: the n-th allocation fails (0 = none) */
+  uint64_t max_buffer_bytes; /* largest single buffer allowed; 0 = the device's free memory */
+  int32_t arithmetic;       /* CELLS_ARITH_FAST (default) or CELLS_ARITH_EXACT */
+  int32_t reserved1;
+} Cells3DConfig;
+
+/* One force sample: ForceSample3 {step, fx, fy, fz} (src/solver3d.ts:33-38), summed in f64. */
+typedef struct {
+  uint32_t step;
+  uint32_t reserved;
+  double fx, fy, fz;
+} CellsForceSample;
+
+typedef struct {
+  int32_t W, H, D, precision;
+  int64_t N;
+  int64_t step;
+  int32_t block_x, block_y; /* launch shape of the step kernel */
+  int32_t force_every;
+  int32_t n_force_blocks;   /* blocks that reduce obstacle forces (0 without a body) */
+} Cells3DInfo;
+
+typedef struct Cells3D Cells3D;
+
+/* ---------------- lifecycle ---------------- */
+
+/* Fills the reference defaults: smagorinsky 0, u_in 0, sponge_fraction 0, sponge_tau 1, absorb 0,
+ * workgroup_size 0 (tuned), force_every 1, lambda NaN, precision FP32, device 0. */
+void cells3d_config_default(Cells3DConfig* cfg);
+
+/* Solver3D.create (src/solver3d.ts:79-104). Checks the size before allocating anything, allocates
+ * every buffer, fills the SDF with FAR = 1e6 and builds the flags. On failure *out is NULL and all
+ * buffers are freed. */
+int cells3d_create(const Cells3DConfig* cfg, Cells3D** out);
+/* Solver3D.destroy (src/solver3d.ts:317-319). NULL is a no-op. */
+void cells3d_destroy(Cells3D* h);
+const char* cells_last_error(const void* handle_or_null);
+
+/* ---------------- setters (src/solver3d.ts:183-194) ---------------- */
+int cells3d_set_tau(Cells3D* h, double tau);               /* setTau */
+int cells3d_set_smagorinsky(Cells3D* h, double cs);        /* setSmagorinsky: stores C_s^2 */
+int cells3d_set_inlet(Cells3D* h, double u);               /* setInlet: already-ramped speed */
+int cells3d_set_lambda(Cells3D* h, double lambda);         /* cfg.lambda; NaN restores trtLambda3(tau) */
+/* Device-side inlet ramp (not in the reference, whose callers ramp on the host between chunks,
+ * src/cases.ts:52-54): before the step that starts at step s the inlet speed is
+ *   target * ramp(min(1, s_q / ramp_steps)),  s_q = s rounded down to a multiple of update_every,
+ * ramp(t) = t (LINEAR) or t*t*(3-2t) (SMOOTHSTEP). update_every = 400 reproduces runRamped's
+ * chunking exactly; 1 ramps every step. kind NONE returns to cells3d_set_inlet. */
+int cells3d_set_inlet_ramp(Cells3D* h, int kind, double target, int64_t ramp_steps, int64_t update_every);
+
+/* ---------------- geometry and state ---------------- */
+/* setSdf (src/solver3d.ts:211-228): copies n = W*H*D floats (cells, negative inside) and rebuilds
+ * flags; cells that stop being solid are refilled from their fluid neighbours. */
+int cells3d_set_sdf(Cells3D* h, const float* sdf, size_t n);
+/* initField (src/solver3d.ts:231-242): every fluid cell to equilibrium at the current inflow speed,
+ * solids to rest; resets step, parity and forces. macro4n (may be NULL) is the 3D macro layout
+ * (ux, uy, uz, rho) per cell and, when given, sets each fluid cell to its own equilibrium
+ * (the 2D reference's initField(macro), src/solver.ts:220-234, extended to 3D). */
+int cells3d_init_field(Cells3D* h, const float* macro4n);
+int cells3d_reset_forces(Cells3D* h);                       /* resetForces */
+
+/* ---------------- stepping ---------------- */
+/* encodeSteps (src/solver3d.ts:252-267): enqueue n steps; returns without waiting. */
+int cells3d_step(Cells3D* h, int64_t n);
+/* encodeMacro (src/solver3d.ts:269-273): refresh the macro buffer from the latest populations. */
+int cells3d_update_macro(Cells3D* h);
+/* run (src/solver3d.ts:276-288): n steps, then the macro refresh, then wait for the GPU. The
+ * reference refreshes the macro after every chunk; only the last refresh is observable, so the
+ * chunk argument only bounds how many steps are enqueued before the host waits. */
+int cells3d_run(Cells3D* h, int64_t n, int64_t chunk);
+int cells3d_synchronize(Cells3D* h);
+
+/* ---------------- readback ---------------- */
+/* readMacro (src/solver3d.ts:290-292): 4N floats (ux, uy, uz, rho), rho = 0 in solids. Waits. */
+int cells3d_read_macro(Cells3D* h, float* out4n);
+/* readForces (src/solver3d.ts:295-315): the samples produced since the last call, oldest first,
+ * at most 8192 (older ones are dropped, as the ring overwrote them). cap must be at least the
+ * number available (8192 always suffices). */
+int cells3d_read_forces(Cells3D* h, CellsForceSample* out, size_t cap, size_t* n_out);
+/* The two halves of readForces, for callers that overlap the copy with other work: begin enqueues
+ * the device-to-host copy; end waits for it. A reset_forces or init_field between the two makes the
+ * read stale: end then returns 0 samples and keeps the later samples aligned (the reference's
+ * generation check, src/solver3d.ts:298-304). */
+int cells3d_read_forces_begin(Cells3D* h);
+int cells3d_read_forces_end(Cells3D* h, CellsForceSample* out, size_t cap, size_t* n_out);
+/* Device-side status bits: 1 = a non-finite force sample, 2 = a non-finite macro value. */
+int cells3d_read_status(Cells3D* h, uint32_t* status);
+int cells3d_get_info(Cells3D* h, Cells3DInfo* info);
+/* The 64-byte Params3 block exactly as the reference packs it (src/shaders/common3d.ts:9-16,
+ * src/solver3d.ts:197-208): u32 W,H,D,N,groupsX,0,0,0; f32 tau, lambda, smagC2, uIn,
+ * spongeStart, tauSponge, absorb, 0. */
+int cells3d_read_params(Cells3D* h, void* out64);
+/* Total mass sum(rho) over fluid cells, accumulated in f64 on the device. Waits. */
+int cells3d_mass(Cells3D* h, double* out);
+/* Raw state access: the latest populations (19*N elements of the storage type), flags (N u32). */
+int cells3d_read_populations(Cells3D* h, void* out, size_t bytes);
+int cells3d_write_populations(Cells3D* h, const void* in, size_t bytes);
+int cells3d_read_flags(Cells3D* h, uint32_t* out, size_t n);
+
+/* ---------------- timing (CUDA events on the handle's stream) ---------------- */
+int cells3d_timer_start(Cells3D* h);
+int cells3d_timer_stop(Cells3D* h, float* ms);
+/* Kernel launches this handle has issued since it was created (graph replays count each node). */
+int cells3d_launch_count(Cells3D* h, int64_t* count);
+
+/* ---------------- fake-device hooks (host-logic tests only) ---------------- */
+/* On a CELLS_FAKE_DEVICE handle, every force sample that a step would reduce is written as
+ * (fx, fy, fz). Any other handle returns CELLS_E_INVALID. */
+int cells3d_fake_set_force(Cells3D* h, double fx, double fy, double fz);
+/* Live fake-device buffers in this process (a failed create must leave this unchanged). */
+int64_t cells_fake_live_buffers(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CELLS_H */

@@ -1,0 +1,31 @@
+"""The C-ABI library loads and exports every function include/cells.h declares (CPU only: no
+compute calls)."""
+import ctypes
+import os
+import re
+
+from cells_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for fn in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if fn.endswith(".h"):
+            src = open(os.path.join(ROOT, "include", fn)).read()
+            src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+            names += re.findall(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(cells\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_the_solver_api():
+    names = declared_functions()
+    for must in ("cells3d_create", "cells3d_step", "cells3d_read_forces", "cells3d_read_macro", "cells3d_set_sdf"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert missing == []

@@ -1,0 +1,196 @@
+"""Parity of the CUDA D3Q19 path (through the C ABI) with the CPU oracle on the same seeded inputs.
+
+Two tolerances:
+  * exact arithmetic (CELLS_ARITH_EXACT): the kernel rounds every operation as written, like the
+    oracle, so stored populations must match bit for bit in every precision;
+  * fast arithmetic (the default, FMA contraction): populations within 2e-6 absolute (f32 storage)
+    after up to 30 steps; force samples within 1e-5 relative.
+Force sums are f64 in both, in different orders: compared to 1e-9 relative in exact mode.
+"""
+import numpy as np
+import pytest
+
+from cells_b200 import Solver3D, geometry as g
+from cells_b200.rng import perturbed_rest3
+from oracle.oracle import OracleSolver3D, decode
+
+pytestmark = pytest.mark.gpu
+
+BASE = dict(tau=0.56, uIn=0.05, spongeFraction=0.15, spongeTau=1.0, absorb=0.02, forceEvery=1)
+
+
+def pair(W, H, D, precision, exact, sdf, **kw):
+    cfg = dict(BASE)
+    cfg.update(kw)
+    s = Solver3D.create(W, H, D, precision=precision, exactArithmetic=exact, **cfg)
+    o = OracleSolver3D(W, H, D, precision, **cfg)
+    s.setSdf(sdf)
+    o.setSdf(sdf)
+    m = perturbed_rest3(W, H, D, 1e-4, ux=cfg["uIn"])
+    s.initField(m)
+    o.initField(m)
+    return s, o
+
+
+def sphere_sdf(W, H, D, cx, cy, cz, r):
+    sdf = g.empty_sdf3(W, H, D)
+    g.add_sphere(sdf, W, H, D, cx, cy, cz, r)
+    return sdf
+
+
+def assert_same(s, o, exact, tol=2e-6):
+    a = s.readPopulations()
+    b = o.populations()
+    assert a.shape == b.shape
+    if exact:
+        bad = np.flatnonzero(a.view(f"u{a.itemsize}") != b.view(f"u{b.itemsize}"))
+        assert bad.size == 0, f"{bad.size} populations differ, first at {bad[:5]}: {a[bad[:5]]} vs {b[bad[:5]]}"
+    else:
+        da, db = decode(a, s.precision), decode(b, s.precision)
+        err = np.max(np.abs(da - db))
+        assert err <= tol, f"max population difference {err}"
+
+
+def assert_forces(fs, fo, rel):
+    assert [x["step"] for x in fs] == [x["step"] for x in fo]
+    for a, b in zip(fs, fo):
+        for k in ("fx", "fy", "fz"):
+            scale = max(abs(b["fx"]), abs(b["fy"]), abs(b["fz"]), 1e-12)
+            assert abs(a[k] - b[k]) <= rel * scale, (a, b)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16", "fp64"])
+def test_sphere_exact_all_precisions(precision):
+    W, H, D = 24, 16, 12
+    s, o = pair(W, H, D, precision, True, sphere_sdf(W, H, D, 8, 8, 6, 3))
+    assert np.array_equal(s.readFlags(), o.flags)
+    for n in (1, 4, 25):
+        s.encodeSteps(n)
+        o.encodeSteps(n)
+        assert_same(s, o, True)
+    assert_forces(s.readForces(), o.readForces(), 1e-9)
+    s.destroy()
+
+
+def test_sphere_fast_fp32_within_tolerance():
+    W, H, D = 24, 16, 12
+    s, o = pair(W, H, D, "fp32", False, sphere_sdf(W, H, D, 8, 8, 6, 3))
+    for n in (1, 29):
+        s.encodeSteps(n)
+        o.encodeSteps(n)
+        assert_same(s, o, False, 2e-6)
+    assert_forces(s.readForces(), o.readForces(), 1e-5)
+    s.run(0)
+    o.run(0)
+    assert np.max(np.abs(s.readMacro() - o.readMacro())) < 1e-5
+    s.destroy()
+
+
+def test_smagorinsky_fixed_lambda_cylinder_touching_slip_faces():
+    """A spanwise cylinder meets both z faces: the slip-face bounce-back with its force branch."""
+    W, H, D = 20, 12, 10
+    sdf = g.empty_sdf3(W, H, D)
+    g.add_cylinder_z(sdf, W, H, D, 7, 6, 2.5)
+    s, o = pair(W, H, D, "fp32", True, sdf, smagorinsky=0.1, lambda_=3 / 16)
+    s.encodeSteps(20)
+    o.encodeSteps(20)
+    assert_same(s, o, True)
+    assert_forces(s.readForces(), o.readForces(), 1e-9)
+    s.destroy()
+
+
+def test_odd_sizes_box_fp64():
+    W, H, D = 19, 7, 5
+    sdf = g.empty_sdf3(W, H, D)
+    g.add_box3(sdf, W, H, D, 6, 3, 2, 1.5, 1.2, 1.0, 0.3)
+    s, o = pair(W, H, D, "fp64", True, sdf, tau=0.8)
+    s.encodeSteps(15)
+    o.encodeSteps(15)
+    assert_same(s, o, True)
+    s.destroy()
+
+
+def test_body_touching_y_face_and_edges():
+    """A sphere cut by the y = 0 face and a box through a z edge: mirrored sources on solids and
+    edge links."""
+    W, H, D = 22, 10, 10
+    sdf = g.empty_sdf3(W, H, D)
+    g.add_sphere(sdf, W, H, D, 8, 0.5, 5, 3)
+    g.add_box3(sdf, W, H, D, 14, 9, 9, 1.5, 1.5, 1.5)
+    s, o = pair(W, H, D, "fp32", True, sdf)
+    s.encodeSteps(12)
+    o.encodeSteps(12)
+    assert_same(s, o, True)
+    assert_forces(s.readForces(), o.readForces(), 1e-9)
+    s.destroy()
+
+
+def test_moved_obstacle_refill():
+    """setSdf after stepping: uncovered cells are refilled from fluid neighbours (aux3d.ts:83-99)."""
+    W, H, D = 24, 12, 12
+    s, o = pair(W, H, D, "fp32", True, sphere_sdf(W, H, D, 8, 6, 6, 3))
+    s.encodeSteps(10)
+    o.encodeSteps(10)
+    moved = sphere_sdf(W, H, D, 11, 6, 6, 3)
+    s.setSdf(moved)
+    o.setSdf(moved)
+    assert np.array_equal(s.readFlags(), o.flags)
+    assert_same(s, o, True)
+    s.encodeSteps(10)
+    o.encodeSteps(10)
+    assert_same(s, o, True)
+    s.destroy()
+
+
+def test_device_ramp_matches_host_ramp():
+    """The device-side smoothstep ramp equals setting u(step) from the host before every step."""
+    W, H, D = 20, 10, 8
+    s, o = pair(W, H, D, "fp32", True, sphere_sdf(W, H, D, 6, 5, 4, 2), uIn=0.0)
+    target, ramp = 0.08, 12
+    s.setInletRamp("smoothstep", target, ramp, 1)
+    for k in range(20):
+        t = min(1.0, k / ramp)
+        o.setInlet(target * (t * t * (3 - 2 * t)))
+        o.encodeSteps(1)
+    s.encodeSteps(20)
+    assert_same(s, o, True)
+    s.destroy()
+
+
+def test_force_every_and_ring_on_device():
+    W, H, D = 20, 10, 8
+    s, o = pair(W, H, D, "fp32", True, sphere_sdf(W, H, D, 6, 5, 4, 2), forceEvery=3)
+    s.encodeSteps(30)
+    o.encodeSteps(30)
+    fs, fo = s.readForces(), o.readForces()
+    assert [x["step"] for x in fs] == list(range(3, 31, 3))
+    assert_forces(fs, fo, 1e-9)
+    s.destroy()
+
+
+def test_mass_and_status():
+    W, H, D = 24, 16, 12
+    s, o = pair(W, H, D, "fp64", True, sphere_sdf(W, H, D, 8, 8, 6, 3))
+    s.encodeSteps(7)
+    o.encodeSteps(7)
+    assert abs(s.mass() - o.mass()) <= 1e-9 * abs(o.mass())
+    assert s.readStatus() == 0
+    s.destroy()
+
+
+def test_config_size_properties():
+    """The 192x96x96 sphere workload of the benchmark: deterministic across runs, finite, no status."""
+    W, H, D = 192, 96, 96
+    sdf = sphere_sdf(W, H, D, 48, 48, 48, 8)
+    res = []
+    for _ in range(2):
+        s = Solver3D.create(W, H, D, precision="fp32", tau=0.524, uIn=0.1, spongeFraction=0.15, absorb=0.02)
+        s.setSdf(sdf)
+        s.initField(perturbed_rest3(W, H, D, 1e-4))
+        s.run(40)
+        res.append((s.readForcesArray(), s.readMacro().copy(), s.readStatus(), s.mass()))
+        s.destroy()
+    (f0, m0, st0, ms0), (f1, m1, st1, ms1) = res
+    assert st0 == 0 and st1 == 0
+    assert np.array_equal(f0, f1) and np.array_equal(m0, m1) and ms0 == ms1
+    assert np.all(np.isfinite(m0)) and f0.shape == (40, 4)

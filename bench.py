@@ -213,7 +213,7 @@ def cpu_baseline(W, H, D, precision="fp32", budget_s=12.0, max_steps=400):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=100)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32")
@@ -280,7 +280,7 @@ def main():
         "vs_baseline": None, "dtype": "f32" if args.precision != "fp64" else "f64", "data": "synthetic",
         "config": {"workload": workload, "grid": [W, H, D], "storage": args.precision, "tau": tau,
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (2 x 134 MB populations)",
-                   "block": [info["block_x"], info["block_y"]], "force_blocks": info["n_force_blocks"]},
+                   "block": [info["block_x"], info["block_y"]], "body_cells": info["n_body_cells"]},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": peak_kind,
                      "bytes_per_cell": BYTES_PER_CELL[args.precision]},

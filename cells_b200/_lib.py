@@ -49,7 +49,7 @@ class Cells3DInfo(C.Structure):
     _fields_ = [
         ("W", C.c_int32), ("H", C.c_int32), ("D", C.c_int32), ("precision", C.c_int32),
         ("N", C.c_int64), ("step", C.c_int64), ("block_x", C.c_int32), ("block_y", C.c_int32),
-        ("force_every", C.c_int32), ("n_force_blocks", C.c_int32),
+        ("force_every", C.c_int32), ("n_body_cells", C.c_int32),
     ]
 
 

@@ -100,6 +100,100 @@ __global__ void flags3_kernel(AuxLaunch3 a, const float* __restrict__ sdf, uint3
   }
 }
 
+// pullSlow3 (src/shaders/step3d.ts:119-168) resolved per (body cell, direction): which source
+// elements a step reads and with which Bouzidi coefficients. q and the coefficients are computed
+// with the reference's operations in the arithmetic type, so the step reproduces its rounding.
+template <class C>
+__global__ void links3_kernel(AuxLaunch3 a, const int* __restrict__ cells, int n, const uint32_t* __restrict__ flags,
+                              const float* __restrict__ sdf, BodyLinks3 L) {
+  using R = typename C::R;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const int W = a.W, H = a.H, D = a.D;
+  const long long N = a.N;
+  const int idx = cells[b];
+  const int WH = W * H;
+  const int z = idx / WH;
+  const int rem = idx - z * WH;
+  const int y = rem / W;
+  const int x = rem - y * W;
+  const uint32_t fl = flags[idx];
+  const bool outlet = (fl & FLAG3_OUTLET) != 0u;
+  L.meta[b] = x | (outlet ? (1 << 29) : 0) | ((fl & FLAG3_INLET) ? (1 << 30) : 0);
+  auto at = [&](int qx, int qy, int qz) { return (long long)qx + (long long)W * (qy + (long long)H * qz); };
+  auto solid = [&](long long cell) { return (flags[cell] & FLAG3_SOLID) != 0u; };
+  Link3<R>* recs = (Link3<R>*)L.rec;
+  unsigned long long kinds = 0ull;
+  for (int i = 1; i < Q3; i++) {
+    const int j = opp3(i);
+    const int sx = x - cx3(i), sy = y - cy3(i), sz = z - cz3(i);
+    uint8_t kind = LINK_LOAD;
+    long long e1 = 0, e2 = -1;
+    R k1 = R(0), k2 = R(0);
+    if ((fl & (1u << i)) == 0u) {
+      e1 = (long long)i * N + at(sx, sy, sz);
+    } else {
+      const bool outX = sx < 0 || sx >= W;
+      const bool outY = sy < 0 || sy >= H;
+      const bool outZ = sz < 0 || sz >= D;
+      if (outX && outlet) {
+        e1 = (long long)i * N + at(W - 2, y, z);
+      } else if (outY && outZ) {
+        e1 = (long long)j * N + idx;
+      } else if (outY || outZ) {
+        const int ry = outY ? y : sy;
+        const int rz = outY ? sz : z;
+        const long long rs = at(sx, ry, rz);
+        if (solid(rs)) {
+          kind = LINK_SLIP_SOLID;
+          e1 = (long long)j * N + idx;
+        } else {
+          e1 = (long long)(outY ? mirror_y3(i) : mirror_z3(i)) * N + rs;
+        }
+      } else if (outX) {
+        e1 = (long long)j * N + idx;
+      } else {
+        const long long s = at(sx, sy, sz);
+        if (!solid(s)) {
+          e1 = (long long)i * N + s;
+        } else {
+          e1 = (long long)j * N + idx;
+          const R dF = R(sdf[idx]);
+          const R dS = R(sdf[s]);
+          R q = dF / max(dF - dS, R(1e-6));
+          q = min(max(q, R(1e-3)), R(1));
+          if (q < R(0.5)) {
+            kind = LINK_BOUZIDI_0;
+            const int nx = x + cx3(i), ny = y + cy3(i), nz = z + cz3(i);
+            if (nx >= 0 && nx < W && ny >= 0 && ny < H && nz >= 0 && nz < D) {
+              const long long nn = at(nx, ny, nz);
+              if (!solid(nn)) {
+                kind = LINK_BOUZIDI_N;
+                e2 = (long long)j * N + nn;
+                k1 = R(2) * q;
+                k2 = R(1) - R(2) * q;
+              }
+            }
+          } else {
+            kind = LINK_BOUZIDI_H;
+            e2 = (long long)i * N + idx;
+            k1 = R(2) * q;
+            k2 = (R(2) * q - R(1)) / (R(2) * q);
+          }
+        }
+      }
+    }
+    Link3<R> rec;
+    rec.e1 = e1;
+    rec.e2 = e2 >= 0 ? e2 : e1;
+    rec.c1 = k1;
+    rec.c2 = k2;
+    recs[(long long)(i - 1) * L.cap + b] = rec;
+    kinds |= (unsigned long long)kind << (3 * (i - 1));
+  }
+  L.kinds[b] = kinds;
+}
+
 template <class C>
 __global__ void init3_kernel(AuxLaunch3 a, typename C::S* __restrict__ fA, typename C::S* __restrict__ fB,
                              const uint32_t* __restrict__ flags, const float4* __restrict__ mac) {
@@ -217,6 +311,13 @@ cudaError_t launch_flags3(int precision, const AuxLaunch3& a, const float* sdf, 
                           void* fA, void* fB, const float4* mac, cudaStream_t s) {
   CELLS_DISPATCH(precision, (flags3_kernel<C><<<blocks_for(a.N, 256), 256, 0, s>>>(
                                 a, sdf, flags, rowBody, (typename C::S*)fA, (typename C::S*)fB, mac)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_links3(int precision, const AuxLaunch3& a, const int* cells, int n, const uint32_t* flags,
+                          const float* sdf, const BodyLinks3& L, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  CELLS_DISPATCH(precision, (links3_kernel<C><<<blocks_for(n, 128), 128, 0, s>>>(a, cells, n, flags, sdf, L)));
   return cudaGetLastError();
 }
 

@@ -46,40 +46,65 @@ __host__ __device__ __forceinline__ R w3(int i) {
   return i == 0 ? R(1) / R(3) : (i <= 6 ? R(1) / R(18) : R(1) / R(36));
 }
 
+template <class R>
+struct Vec4;
+template <>
+struct Vec4<float> {
+  using T = float4;
+};
+template <>
+struct Vec4<double> {
+  using T = double4;
+};
+
 // ---------------- storage codecs ----------------
+// load/enc convert between stored values and populations (f_i - w_i). raw/enc_raw work in storage
+// units, populations times SCALE: the step kernel computes in those units, which is exact because
+// SCALE is a power of two, so it gives the same bits as scaling every load and store.
 struct CodecF32 {
   using S = float;
   using R = float;
   static constexpr int prec = 0;
+  static constexpr float SCALE = 1.0f;
   __device__ __forceinline__ static R load(const S* p) { return __ldg(p); }
-  __device__ __forceinline__ static R cvt(S v) { return v; }
   __device__ __forceinline__ static S enc(R v) { return v; }
+  __device__ __forceinline__ static R raw(const S* p) { return __ldg(p); }
+  __device__ __forceinline__ static S enc_raw(R v) { return v; }
 };
 struct CodecF16 {
   using S = __half;
   using R = float;
   static constexpr int prec = 1;
-  __device__ __forceinline__ static R cvt(S v) { return __half2float(v) * (1.0f / 32768.0f); }
-  __device__ __forceinline__ static R load(const S* p) { return cvt(__ldg(p)); }
+  static constexpr float SCALE = 32768.0f;
+  __device__ __forceinline__ static R load(const S* p) { return __half2float(__ldg(p)) * (1.0f / 32768.0f); }
   __device__ __forceinline__ static S enc(R v) {
     return __float2half_rn(fminf(fmaxf(v, -1.99f), 1.99f) * 32768.0f);
+  }
+  __device__ __forceinline__ static R raw(const S* p) { return __half2float(__ldg(p)); }
+  // clamp(v, -1.99, 1.99) * 2^15 == clamp(v * 2^15, -1.99 * 2^15, 1.99 * 2^15): both products are exact
+  __device__ __forceinline__ static S enc_raw(R v) {
+    return __float2half_rn(fminf(fmaxf(v, -1.99f * 32768.0f), 1.99f * 32768.0f));
   }
 };
 struct CodecBF16 {
   using S = __nv_bfloat16;
   using R = float;
   static constexpr int prec = 2;
-  __device__ __forceinline__ static R cvt(S v) { return __bfloat162float(v); }
-  __device__ __forceinline__ static R load(const S* p) { return cvt(__ldg(p)); }
+  static constexpr float SCALE = 1.0f;
+  __device__ __forceinline__ static R load(const S* p) { return __bfloat162float(__ldg(p)); }
   __device__ __forceinline__ static S enc(R v) { return __float2bfloat16_rn(v); }
+  __device__ __forceinline__ static R raw(const S* p) { return __bfloat162float(__ldg(p)); }
+  __device__ __forceinline__ static S enc_raw(R v) { return __float2bfloat16_rn(v); }
 };
 struct CodecF64 {
   using S = double;
   using R = double;
   static constexpr int prec = 3;
+  static constexpr double SCALE = 1.0;
   __device__ __forceinline__ static R load(const S* p) { return __ldg(p); }
-  __device__ __forceinline__ static R cvt(S v) { return v; }
   __device__ __forceinline__ static S enc(R v) { return v; }
+  __device__ __forceinline__ static R raw(const S* p) { return __ldg(p); }
+  __device__ __forceinline__ static S enc_raw(R v) { return v; }
 };
 
 // Per-handle device state. step[] and uIn[] are double-buffered by parity: the step kernel of

@@ -109,6 +109,21 @@ void* Device::host_pinned(size_t bytes) {
   return p;
 }
 
+void Device::release(void* d) {
+  if (!d) return;
+  for (size_t k = 0; k < owned.size(); k++) {
+    if (owned[k] != d) continue;
+    owned.erase(owned.begin() + (long)k);
+    if (fake) {
+      std::free(d);
+      g_fake_live_buffers--;
+    } else {
+      cudaFree(d);
+    }
+    return;
+  }
+}
+
 void Device::free_host_pinned(void* p) {
   if (!p) return;
   if (fake) {

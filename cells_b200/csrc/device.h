@@ -45,6 +45,7 @@ struct Device {
   void sync();
   void* host_pinned(size_t bytes);
   void free_host_pinned(void* p);
+  void release(void* d);  // frees one buffer from alloc() before close()
   size_t free_bytes();
 };
 

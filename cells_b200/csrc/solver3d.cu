@@ -5,6 +5,7 @@
 // encodeSteps (:252-267), run (:276-288), readMacro (:290-292) and readForces with its ring window
 // and generation check (:295-315). Everything is enqueued on the handle's own CUDA stream.
 #include <cmath>
+#include <cstdlib>
 #include <deque>
 #include <mutex>
 #include <string>
@@ -35,8 +36,8 @@ struct Cells3D {
   float* sdf = nullptr;
   uint8_t* rowBody = nullptr;
   void* xTab = nullptr;
-  int* blockSlot = nullptr;
-  double4* partials = nullptr;
+  int* bodyCells = nullptr;  // capacity N
+  double4* partials = nullptr;  // one per body block
   double4* history = nullptr;
   DevState3* st = nullptr;
   float4* macro = nullptr;
@@ -50,7 +51,8 @@ struct Cells3D {
   uint64_t forceSamplesRead = 0;
   std::deque<uint32_t> forceSteps;
   uint64_t forceGeneration = 0;
-  int nForceBlocks = 1;
+  int nBody = 0;
+  BodyLinks3 links{};
 
   // inlet
   double uIn = 0.0;
@@ -84,7 +86,7 @@ struct Cells3D {
   void choose_launch();
   void upload_xtab();
   void rebuild_flags();
-  void build_block_slots(const std::vector<uint8_t>& rows);
+  void build_body_list(const std::vector<uint8_t>& rows);
   void launch_steps(int64_t n);
   void write_state(int which);
   void free_all();
@@ -92,13 +94,15 @@ struct Cells3D {
 
 // ---------------- helpers ----------------
 
+// Per-x table (omega+ without Smagorinsky, omega-, sigma, 0). The reference computes these per
+// cell in f32 (src/shaders/step3d.ts:72-74 and :213-219); the same f32 operations in the same order
+// give the same values here (the host build does not contract multiply-adds).
 template <class R>
-static void fill_xtab(std::vector<R>& t, int W, double tau, double spongeStart, double tauSponge, double absorb) {
-  // The reference computes these per cell in f32 (src/shaders/step3d.ts:213-219); the same f32
-  // operations in the same order give the same values here (no FMA contraction on the host).
-  const R tauR = (R)tau, ssR = (R)spongeStart, tsR = (R)tauSponge, abR = (R)absorb;
+static void fill_xtab(std::vector<R>& t, int W, double tau, double lambda, double spongeStart, double tauSponge,
+                      double absorb) {
+  const R tauR = (R)tau, lamR = (R)lambda, ssR = (R)spongeStart, tsR = (R)tauSponge, abR = (R)absorb;
   const R e1 = (R)(W - 1);
-  t.resize(2 * (size_t)W);
+  t.resize(4 * (size_t)W);
   for (int x = 0; x < W; x++) {
     R omegaBase = R(1) / tauR;
     R sOut = R(0);
@@ -109,8 +113,10 @@ static void fill_xtab(std::vector<R>& t, int W, double tau, double spongeStart, 
       const R mix = tauR * (R(1) - sOut) + tsR * sOut;
       omegaBase = R(1) / mix;
     }
-    t[2 * x] = omegaBase;
-    t[2 * x + 1] = abR * sOut * sOut;
+    t[4 * x] = omegaBase;
+    t[4 * x + 1] = R(1) / (R(0.5) + lamR / (R(1) / omegaBase - R(0.5)));
+    t[4 * x + 2] = abR * sOut * sOut;
+    t[4 * x + 3] = R(0);
   }
 }
 
@@ -141,11 +147,11 @@ void Cells3D::choose_launch() {
 void Cells3D::upload_xtab() {
   if (prec == 3) {
     std::vector<double> t;
-    fill_xtab<double>(t, W, cfg.tau, sponge_start(), tau_sponge(), cfg.absorb);
+    fill_xtab<double>(t, W, cfg.tau, lambda_value(), sponge_start(), tau_sponge(), cfg.absorb);
     dev.h2d(xTab, t.data(), t.size() * sizeof(double));
   } else {
     std::vector<float> t;
-    fill_xtab<float>(t, W, cfg.tau, sponge_start(), tau_sponge(), cfg.absorb);
+    fill_xtab<float>(t, W, cfg.tau, lambda_value(), sponge_start(), tau_sponge(), cfg.absorb);
     dev.h2d(xTab, t.data(), t.size() * sizeof(float));
   }
   if (!dev.fake) dev.sync();  // the host vectors die here
@@ -165,25 +171,47 @@ void Cells3D::write_state(int which) {
   dev.launches++;
 }
 
-void Cells3D::build_block_slots(const std::vector<uint8_t>& rows) {
-  std::vector<int> slots((size_t)nBlocks, -1);
-  int k = 0;
-  for (int z = 0; z < D; z++)
-    for (int byi = 0; byi < gy; byi++) {
-      bool body = false;
-      for (int y = byi * by; y < std::min(H, (byi + 1) * by); y++) body = body || rows[(size_t)y + (size_t)H * z];
-      for (int bxi = 0; bxi < gx; bxi++) {
-        const size_t b = (size_t)bxi + (size_t)gx * ((size_t)byi + (size_t)gy * z);
-        if (body || b == 0) slots[b] = k++;
+// The body kernel's cells: every fluid cell with a non-zero flag in a row that holds a body cell,
+// in increasing index order (so the force reduction order is fixed).
+void Cells3D::build_body_list(const std::vector<uint8_t>& rows) {
+  std::vector<int> cells;
+  if (!dev.fake) {
+    std::vector<uint32_t> fl((size_t)N);
+    dev.d2h(fl.data(), flags, (size_t)N * 4);
+    dev.sync();
+    for (int z = 0; z < D; z++)
+      for (int y = 0; y < H; y++) {
+        if (!rows[(size_t)y + (size_t)H * z]) continue;
+        const size_t base = (size_t)W * ((size_t)y + (size_t)H * z);
+        for (int x = 0; x < W; x++)
+          if (fl[base + x] != 0u && !(fl[base + x] & FLAG3_SOLID)) cells.push_back((int)(base + x));
       }
-    }
-  nForceBlocks = k;
-  dev.h2d(blockSlot, slots.data(), slots.size() * sizeof(int));
-  if (!dev.fake) dev.sync();
+  }
+  nBody = (int)cells.size();
+  if (nBody > 0) {
+    dev.h2d(bodyCells, cells.data(), cells.size() * sizeof(int));
+    dev.sync();
+  }
+  if (nBody > links.cap) {
+    // grow the link tables (18 links per body cell)
+    for (void* p : {links.rec, (void*)links.kinds, (void*)links.meta}) dev.release(p);
+    links = BodyLinks3{};
+    const int cap = std::max(nBody, 4096);
+    links.rec = dev.alloc(18 * (size_t)cap * 32, "body links");  // sizeof(Link3<R>) is 32 for f32 and f64
+    links.kinds = (unsigned long long*)dev.alloc((size_t)cap * 8, "body links");
+    links.meta = (int*)dev.alloc((size_t)cap * 4, "body links");
+    links.cap = cap;
+  }
+  if (nBody > 0 && !dev.fake) {
+    AuxLaunch3 a{W, H, D, (int)N, current_uin()};
+    check_cuda(launch_links3(prec, a, bodyCells, nBody, flags, sdf, links, dev.stream), "links kernel");
+    dev.launches++;
+    dev.sync();
+  }
 }
 
 // rebuildFlags, src/solver3d.ts:216-228: a macro pass on the latest populations (the refill reads
-// it), then the flags pass, then the body-row map that picks the force blocks.
+// it), then the flags pass, then the body-row map and the body cell list.
 void Cells3D::rebuild_flags() {
   std::vector<uint8_t> rows((size_t)H * D, 0);
   if (!dev.fake) {
@@ -196,7 +224,7 @@ void Cells3D::rebuild_flags() {
     dev.d2h(rows.data(), rowBody, rows.size());
     dev.sync();
   }
-  build_block_slots(rows);
+  build_body_list(rows);
 }
 
 void Cells3D::launch_steps(int64_t n) {
@@ -217,17 +245,18 @@ void Cells3D::launch_steps(int64_t n) {
       a.sdf = sdf;
       a.rowBody = rowBody;
       a.xTab = xTab;
-      a.blockSlot = blockSlot;
+      a.bodyCells = bodyCells;
+      a.links = links;
       a.partials = partials;
       a.history = history;
       a.st = st;
       a.W = W;
       a.H = H;
       a.D = D;
-      a.N = (int)N;
+      a.N = N;
       a.bx = bx;
       a.by = by;
-      a.nForceBlocks = nForceBlocks;
+      a.nBody = nBody;
       a.rampKind = rampKind;
       a.rampEvery = (int)rampEvery;
       a.rampTarget = rampTarget;
@@ -238,8 +267,8 @@ void Cells3D::launch_steps(int64_t n) {
       a.sample = sample ? 1 : 0;
       check_cuda(cfg.arithmetic == CELLS_ARITH_EXACT ? exact::launch_step3(prec, a, dev.stream)
                                                      : fast::launch_step3(prec, a, dev.stream),
-                 "step kernel");
-      dev.launches++;
+                 "step kernels");
+      dev.launches += (nBody > 0 || sample) ? 2 : 1;
     }
     parity ^= 1;
     step++;
@@ -353,9 +382,9 @@ int cells3d_create(const Cells3DConfig* cfg, Cells3D** out) {
     h->sdf = (float*)h->dev.alloc((size_t)N * 4, "sdf");
     h->macro = (float4*)h->dev.alloc((size_t)N * 16, "macro");
     h->rowBody = (uint8_t*)h->dev.alloc((size_t)h->H * h->D, "row map");
-    h->xTab = h->dev.alloc((size_t)h->W * 2 * (h->prec == 3 ? 8 : 4), "x table");
-    h->blockSlot = (int*)h->dev.alloc((size_t)h->nBlocks * 4, "block slots");
-    h->partials = (double4*)h->dev.alloc((size_t)h->nBlocks * sizeof(double4), "force partials");
+    h->xTab = h->dev.alloc((size_t)h->W * 4 * (h->prec == 3 ? 8 : 4), "x table");
+    h->bodyCells = (int*)h->dev.alloc((size_t)N * 4, "body cell list");
+    h->partials = (double4*)h->dev.alloc((size_t)(N / 32 + 2) * sizeof(double4), "force partials");
     h->history = (double4*)h->dev.alloc((size_t)HISTORY_LEN * sizeof(double4), "force history");
     h->st = (DevState3*)h->dev.alloc(sizeof(DevState3), "state");
     h->nMassPartials = 4 * 148;
@@ -419,8 +448,10 @@ int cells3d_set_smagorinsky(Cells3D* h, double cs) {
 
 int cells3d_set_lambda(Cells3D* h, double lambda) {
   if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
   h->cfg.lambda = lambda;
-  return CELLS_OK;
+  h->upload_xtab();
+  CELLS_CATCH(h)
 }
 
 int cells3d_set_inlet(Cells3D* h, double u) {
@@ -626,7 +657,7 @@ int cells3d_get_info(Cells3D* h, Cells3DInfo* info) {
   info->block_x = h->bx;
   info->block_y = h->by;
   info->force_every = h->cfg.force_every;
-  info->n_force_blocks = h->nForceBlocks;
+  info->n_body_cells = h->nBody;
   return CELLS_OK;
 }
 

@@ -94,7 +94,7 @@ typedef struct {
   int64_t step;
   int32_t block_x, block_y; /* launch shape of the step kernel */
   int32_t force_every;
-  int32_t n_force_blocks;   /* blocks that reduce obstacle forces (0 without a body) */
+  int32_t n_body_cells;     /* cells the body kernel updates (fluid cells with a flag in rows with a body) */
 } Cells3DInfo;
 
 typedef struct Cells3D Cells3D;

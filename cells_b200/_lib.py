@@ -105,6 +105,7 @@ def lib() -> C.CDLL:
         "cells3d_launch_count": (I, [P, C.POINTER(I64)]),
         "cells3d_fake_set_force": (I, [P, D, D, D]),
         "cells_fake_live_buffers": (I64, []),
+        "cells3d_mass_noalloc": (I, [P, P, I64, C.c_int32, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

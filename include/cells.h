@@ -174,6 +174,20 @@ int cells3d_read_populations(Cells3D* h, void* out, size_t bytes);
 int cells3d_write_populations(Cells3D* h, const void* in, size_t bytes);
 int cells3d_read_flags(Cells3D* h, uint32_t* out, size_t n);
 
+/* Allocation-free mass reduction. It has no counterpart in the reference. It is for callers that
+ * cannot allocate device memory when they need the result: code inside a CUDA stream capture,
+ * hosts that fix their device memory at start-up, real-time loops that must not risk the failure
+ * or the implicit synchronisation of cudaMalloc/cudaFree. The caller passes device pointers to
+ * the populations (19 * n_cells values of the storage type, layout f[i * n_cells + cell]) and to
+ * the flags (n_cells u32), a device pointer for the f64 result, and a CUDA stream (NULL = the
+ * default stream); the call enqueues the work and returns without waiting. The partial sums live in
+ * a fixed 64 KiB __device__ array, one partial per 8192 cells: grids above 67,108,864 cells are
+ * rejected with CELLS_E_INVALID. Calls share that array, so calls that can overlap on the GPU
+ * race and must be serialised by the caller. The first call on a device looks up the array's
+ * address and should come before any stream capture. Errors: cells_last_error(NULL). */
+int cells3d_mass_noalloc(const void* populations, const uint32_t* flags, int64_t n_cells, int32_t precision,
+                         double* out_device, void* stream);
+
 /* ---------------- timing (CUDA events on the handle's stream) ---------------- */
 int cells3d_timer_start(Cells3D* h);
 int cells3d_timer_stop(Cells3D* h, float* ms);

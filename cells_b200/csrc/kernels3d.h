@@ -55,15 +55,23 @@ struct StepLaunch3 {
   int par, sample;
 };
 
-// One time step: the bulk kernel, then the body kernel when there are body cells or the step is
-// sampled. precision: cells_precision (0 f32, 1 f16, 2 bf16, 3 f64). fast: FMA contraction
-// allowed; exact: no contraction, every operation rounds as written.
+// Streams of one step: the bulk kernel runs on main; the body kernel runs on side (forked from and
+// joined back into main with the two events), or on main after the bulk kernel when side is null.
+struct StepStreams3 {
+  cudaStream_t main;
+  cudaStream_t side;
+  cudaEvent_t fork, join;
+};
+
+// One time step: the bulk kernel and, when there are body cells or the step is sampled, the body
+// kernel. precision: cells_precision (0 f32, 1 f16, 2 bf16, 3 f64). fast: FMA contraction allowed;
+// exact: no contraction, every operation rounds as written.
 namespace fast {
-cudaError_t launch_step3(int precision, const StepLaunch3& a, cudaStream_t s);
+cudaError_t launch_step3(int precision, const StepLaunch3& a, const StepStreams3& ss);
 int body_blocks3(int nBody);
 }
 namespace exact {
-cudaError_t launch_step3(int precision, const StepLaunch3& a, cudaStream_t s);
+cudaError_t launch_step3(int precision, const StepLaunch3& a, const StepStreams3& ss);
 int body_blocks3(int nBody);
 }
 

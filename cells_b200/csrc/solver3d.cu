@@ -83,10 +83,27 @@ struct Cells3D {
   }
   double current_uin() const { return rampKind ? ramp_speed(step) : uIn; }
 
+  // CUDA graphs of kGraphSteps steps, one per phase of the launch-argument period; argGen counts
+  // changes of the arguments the graphs bake in (parameters, ramp, body links), so a stale graph is
+  // rebuilt on its next use. CELLS_GRAPHS=0 in the environment launches every step directly.
+  struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t gen = 0;
+    int launches = 0;
+  };
+  static constexpr int kGraphSteps = 128;
+  static constexpr int kMaxGraphPeriod = 16;
+  std::vector<StepGraph> graphs = std::vector<StepGraph>(kMaxGraphPeriod);
+  uint64_t argGen = 1;
+  bool useGraphs = true;
+
   void choose_launch();
   void upload_xtab();
   void rebuild_flags();
   void build_body_list(const std::vector<uint8_t>& rows);
+  int enqueue_step(int par, bool sample, cudaStream_t main);
+  int graph_period() const;
+  void build_graph(int phase);
   void launch_steps(int64_t n);
   void write_state(int which);
   void free_all();
@@ -225,11 +242,96 @@ void Cells3D::rebuild_flags() {
     dev.sync();
   }
   build_body_list(rows);
+  argGen++;  // the body list and links are baked into step graphs
+}
+
+// Enqueues the kernels of one step of parity par on `main` (plus the side stream for the body
+// kernel) and returns how many kernels it launched.
+int Cells3D::enqueue_step(int par, bool sample, cudaStream_t main) {
+  StepLaunch3 a;
+  a.src = f[par];
+  a.dst = f[par ^ 1];
+  a.flags = flags;
+  a.sdf = sdf;
+  a.rowBody = rowBody;
+  a.xTab = xTab;
+  a.bodyCells = bodyCells;
+  a.links = links;
+  a.partials = partials;
+  a.history = history;
+  a.st = st;
+  a.W = W;
+  a.H = H;
+  a.D = D;
+  a.N = N;
+  a.bx = bx;
+  a.by = by;
+  a.nBody = nBody;
+  a.rampKind = rampKind;
+  a.rampEvery = (int)rampEvery;
+  a.rampTarget = rampTarget;
+  a.rampSteps = (double)rampSteps;
+  a.lambda = lambda_value();
+  a.smagC2 = cfg.smagorinsky * cfg.smagorinsky;
+  a.par = par;
+  a.sample = sample ? 1 : 0;
+  const StepStreams3 ss{main, dev.side, dev.evFork, dev.evJoin};
+  check_cuda(cfg.arithmetic == CELLS_ARITH_EXACT ? exact::launch_step3(prec, a, ss) : fast::launch_step3(prec, a, ss),
+             "step kernels");
+  return (nBody > 0 || sample) ? 2 : 1;
+}
+
+// Steps repeat with period lcm(2, force_every) in their launch arguments (parity and sampling);
+// graphs are kept per phase of that period. Longer periods run without graphs.
+int Cells3D::graph_period() const {
+  const int every = cfg.force_every;
+  if (every <= 0) return 2;
+  return (every % 2 == 0) ? every : 2 * every;
+}
+
+void Cells3D::build_graph(int phase) {
+  StepGraph& g = graphs[phase];
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  g.exec = nullptr;
+  const int every = cfg.force_every;
+  int launches = 0;
+  check_cuda(cudaStreamBeginCapture(dev.stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  int par = phase % 2;
+  int64_t s = phase;
+  for (int k = 0; k < kGraphSteps; k++) {
+    const bool sample = every > 0 && ((s + 1) % every) == 0;
+    launches += enqueue_step(par, sample, dev.stream);
+    par ^= 1;
+    s++;
+  }
+  cudaGraph_t graph = nullptr;
+  check_cuda(cudaStreamEndCapture(dev.stream, &graph), "cudaStreamEndCapture");
+  cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  check_cuda(e, "cudaGraphInstantiate");
+  g.gen = argGen;
+  g.launches = launches;
 }
 
 void Cells3D::launch_steps(int64_t n) {
   const int every = cfg.force_every;
-  for (int64_t k = 0; k < n; k++) {
+  const int period = graph_period();
+  while (n > 0) {
+    if (!dev.fake && useGraphs && period <= kMaxGraphPeriod && n >= kGraphSteps) {
+      // kGraphSteps steps as one graph launch: parity and sampling depend on step % period only
+      const int phase = (int)(step % period);
+      if (!graphs[phase].exec || graphs[phase].gen != argGen) build_graph(phase);
+      check_cuda(cudaGraphLaunch(graphs[phase].exec, dev.stream), "cudaGraphLaunch");
+      dev.launches += graphs[phase].launches;
+      for (int k = 0; k < kGraphSteps; k++) {
+        const bool sample = every > 0 && ((step + 1) % every) == 0;
+        parity ^= 1;
+        step++;
+        if (sample) forceSteps.push_back((uint32_t)step);
+      }
+      n -= kGraphSteps;
+      continue;
+    }
     const bool sample = every > 0 && ((step + 1) % every) == 0;
     if (dev.fake) {
       if (sample) {
@@ -238,45 +340,19 @@ void Cells3D::launch_steps(int64_t n) {
         st->sample = s + 1;
       }
     } else {
-      StepLaunch3 a;
-      a.src = f[parity];
-      a.dst = f[parity ^ 1];
-      a.flags = flags;
-      a.sdf = sdf;
-      a.rowBody = rowBody;
-      a.xTab = xTab;
-      a.bodyCells = bodyCells;
-      a.links = links;
-      a.partials = partials;
-      a.history = history;
-      a.st = st;
-      a.W = W;
-      a.H = H;
-      a.D = D;
-      a.N = N;
-      a.bx = bx;
-      a.by = by;
-      a.nBody = nBody;
-      a.rampKind = rampKind;
-      a.rampEvery = (int)rampEvery;
-      a.rampTarget = rampTarget;
-      a.rampSteps = (double)rampSteps;
-      a.lambda = lambda_value();
-      a.smagC2 = cfg.smagorinsky * cfg.smagorinsky;
-      a.par = parity;
-      a.sample = sample ? 1 : 0;
-      check_cuda(cfg.arithmetic == CELLS_ARITH_EXACT ? exact::launch_step3(prec, a, dev.stream)
-                                                     : fast::launch_step3(prec, a, dev.stream),
-                 "step kernels");
-      dev.launches += (nBody > 0 || sample) ? 2 : 1;
+      dev.launches += enqueue_step(parity, sample, dev.stream);
     }
     parity ^= 1;
     step++;
     if (sample) forceSteps.push_back((uint32_t)step);
+    n--;
   }
 }
 
 void Cells3D::free_all() {
+  for (auto& g : graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  graphs.assign(kMaxGraphPeriod, StepGraph{});
   if (stageHist) dev.free_host_pinned(stageHist);
   if (stageState) dev.free_host_pinned(stageState);
   stageHist = nullptr;
@@ -361,6 +437,7 @@ int cells3d_create(const Cells3DConfig* cfg, Cells3D** out) {
   h->prec = cfg->precision;
   h->bpp = h->prec == 0 ? 4 : (h->prec == 3 ? 8 : 2);
   h->uIn = cfg->u_in;
+  if (const char* gv = std::getenv("CELLS_GRAPHS")) h->useGraphs = std::atoi(gv) != 0;
   try {
     h->dev.open(cfg->device, cfg->fake_fail_alloc);
     const unsigned long long fBytes = 19ull * h->bpp * (unsigned long long)N;
@@ -436,6 +513,7 @@ int cells3d_set_tau(Cells3D* h, double tau) {
   CELLS_TRY(h)
   if (!(tau > 0.5)) throw Error(CELLS_E_INVALID, "tau must be above 1/2");
   h->cfg.tau = tau;
+  h->argGen++;
   h->upload_xtab();
   CELLS_CATCH(h)
 }
@@ -443,6 +521,7 @@ int cells3d_set_tau(Cells3D* h, double tau) {
 int cells3d_set_smagorinsky(Cells3D* h, double cs) {
   if (!h) return CELLS_E_INVALID;
   h->cfg.smagorinsky = cs;
+  h->argGen++;
   return CELLS_OK;
 }
 
@@ -450,6 +529,7 @@ int cells3d_set_lambda(Cells3D* h, double lambda) {
   if (!h) return CELLS_E_INVALID;
   CELLS_TRY(h)
   h->cfg.lambda = lambda;
+  h->argGen++;
   h->upload_xtab();
   CELLS_CATCH(h)
 }
@@ -471,6 +551,7 @@ int cells3d_set_inlet_ramp(Cells3D* h, int kind, double target, int64_t ramp_ste
   if (kind != 0 && (ramp_steps <= 0 || update_every <= 0))
     throw Error(CELLS_E_INVALID, "ramp_steps and update_every must be positive");
   h->rampKind = kind;
+  h->argGen++;
   h->rampTarget = target;
   h->rampSteps = ramp_steps > 0 ? ramp_steps : 1;
   h->rampEvery = update_every > 0 ? update_every : 1;

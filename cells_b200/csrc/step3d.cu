@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(32 * Q3) body3d_kernel(const __grid_constant__
 int body_blocks3(int nBody);
 
 template <class C>
-static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
+static cudaError_t launch_step3_t(const StepLaunch3& L, const StepStreams3& ss) {
   using R = typename C::R;
   using S = typename C::S;
   StepArgs3<C> a;
@@ -446,32 +446,42 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   dim3 block(L.bx, L.by, 1);
   dim3 grid((L.W + L.bx - 1) / L.bx, (L.H + L.by - 1) / L.by, L.D);
   const bool smag = L.smagC2 > 0;
-  if (smag)
-    bulk3d_kernel<C, true><<<grid, block, 0, s>>>(a);
-  else
-    bulk3d_kernel<C, false><<<grid, block, 0, s>>>(a);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  cudaError_t e;
   // the body kernel runs when there are body cells, and on sampled steps even without them (a
-  // sample of zero force is still written to the ring, as the reference's reduce pass does)
-  if (L.nBody > 0 || L.sample) {
+  // sample of zero force is still written to the ring, as the reference's reduce pass does). The
+  // two kernels touch disjoint cells, so the body kernel runs on a side stream beside the bulk one.
+  const bool body = L.nBody > 0 || L.sample;
+  const bool side = body && ss.side != nullptr;
+  cudaStream_t bs = side ? ss.side : ss.main;
+  if (side) {
+    if ((e = cudaEventRecord(ss.fork, ss.main)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ss.side, ss.fork, 0)) != cudaSuccess) return e;
+  }
+  if (body) {
     const int blocks = body_blocks3(L.nBody);
     const dim3 bblock(32, Q3, 1);
     if (smag)
-      body3d_kernel<C, true><<<blocks, bblock, 0, s>>>(a);
+      body3d_kernel<C, true><<<blocks, bblock, 0, bs>>>(a);
     else
-      body3d_kernel<C, false><<<blocks, bblock, 0, s>>>(a);
-    e = cudaGetLastError();
+      body3d_kernel<C, false><<<blocks, bblock, 0, bs>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
+  if (side && (e = cudaEventRecord(ss.join, ss.side)) != cudaSuccess) return e;
+  if (smag)
+    bulk3d_kernel<C, true><<<grid, block, 0, ss.main>>>(a);
+  else
+    bulk3d_kernel<C, false><<<grid, block, 0, ss.main>>>(a);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (side) e = cudaStreamWaitEvent(ss.main, ss.join, 0);
   return e;
 }
 
-cudaError_t launch_step3(int precision, const StepLaunch3& a, cudaStream_t s) {
+cudaError_t launch_step3(int precision, const StepLaunch3& a, const StepStreams3& ss) {
   switch (precision) {
-    case 0: return launch_step3_t<CodecF32>(a, s);
-    case 1: return launch_step3_t<CodecF16>(a, s);
-    case 2: return launch_step3_t<CodecBF16>(a, s);
-    case 3: return launch_step3_t<CodecF64>(a, s);
+    case 0: return launch_step3_t<CodecF32>(a, ss);
+    case 1: return launch_step3_t<CodecF16>(a, ss);
+    case 2: return launch_step3_t<CodecBF16>(a, ss);
+    case 3: return launch_step3_t<CodecF64>(a, ss);
   }
   return cudaErrorInvalidValue;
 }

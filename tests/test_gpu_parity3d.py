@@ -194,3 +194,24 @@ def test_config_size_properties():
     assert st0 == 0 and st1 == 0
     assert np.array_equal(f0, f1) and np.array_equal(m0, m1) and ms0 == ms1
     assert np.all(np.isfinite(m0)) and f0.shape == (40, 4)
+
+
+@pytest.mark.parametrize("every", [1, 3, 4])
+def test_graph_replay_matches_oracle(every):
+    """Long step runs replay cached CUDA graphs (128 steps each, one per phase of the parity and
+    sampling period); a parameter change between replays rebuilds them."""
+    W, H, D = 20, 10, 8
+    s, o = pair(W, H, D, "fp32", True, sphere_sdf(W, H, D, 6, 5, 4, 2), forceEvery=every)
+    for n in (5, 260, 131):
+        s.encodeSteps(n)
+        o.encodeSteps(n)
+    assert_same(s, o, True)
+    assert_forces(s.readForces(), o.readForces(), 1e-9)
+    s.setTau(0.6)
+    o.setTau(0.6)
+    s.encodeSteps(200)
+    o.encodeSteps(200)
+    assert_same(s, o, True)
+    assert_forces(s.readForces(), o.readForces(), 1e-9)
+    assert s.launchCount() > 2 * 596  # every step launched the bulk kernel and most the body kernel
+    s.destroy()

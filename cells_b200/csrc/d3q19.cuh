@@ -85,6 +85,17 @@ struct CodecF16 {
   __device__ __forceinline__ static S enc_raw(R v) {
     return __float2half_rn(fminf(fmaxf(v, -1.99f * 32768.0f), 1.99f * 32768.0f));
   }
+  // Two values in the halves of one 32-bit word (lo = first cell). Rounding first and clamping the
+  // halves to +-65216 gives the same bits as enc_raw: 65216 is the f16 nearest to 1.99 * 2^15, and
+  // rounding is monotonic, so every value beyond the clamp bound rounds to 65216 or further out.
+  __device__ __forceinline__ static R lo(uint32_t w) { return __half2float(__ushort_as_half((unsigned short)w)); }
+  __device__ __forceinline__ static R hi(uint32_t w) { return __half2float(__ushort_as_half((unsigned short)(w >> 16))); }
+  __device__ __forceinline__ static uint32_t pack2(R a, R b) {
+    __half2 h = __floats2half2_rn(a, b);
+    const __half2 bound = __float2half2_rn(65216.0f);
+    h = __hmin2(__hmax2(h, __hneg2(bound)), bound);
+    return *reinterpret_cast<uint32_t*>(&h);
+  }
 };
 struct CodecBF16 {
   using S = __nv_bfloat16;
@@ -95,6 +106,12 @@ struct CodecBF16 {
   __device__ __forceinline__ static S enc(R v) { return __float2bfloat16_rn(v); }
   __device__ __forceinline__ static R raw(const S* p) { return __bfloat162float(__ldg(p)); }
   __device__ __forceinline__ static S enc_raw(R v) { return __float2bfloat16_rn(v); }
+  __device__ __forceinline__ static R lo(uint32_t w) { return __uint_as_float(w << 16); }
+  __device__ __forceinline__ static R hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
+  __device__ __forceinline__ static uint32_t pack2(R a, R b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&h);
+  }
 };
 struct CodecF64 {
   using S = double;

@@ -29,9 +29,6 @@ void Device::open(int device_ordinal, int fail_alloc_at) {
   check_cuda(cudaEventCreate(&ev0), "cudaEventCreate");
   check_cuda(cudaEventCreate(&ev1), "cudaEventCreate");
   check_cuda(cudaEventCreateWithFlags(&evRead, cudaEventDisableTiming), "cudaEventCreate");
-  check_cuda(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "cudaStreamCreate");
-  check_cuda(cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming), "cudaEventCreate");
-  check_cuda(cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming), "cudaEventCreate");
 }
 
 void Device::close() {
@@ -49,15 +46,9 @@ void Device::close() {
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (evRead) cudaEventDestroy(evRead);
-  if (evFork) cudaEventDestroy(evFork);
-  if (evJoin) cudaEventDestroy(evJoin);
-  if (side) {
-    cudaStreamSynchronize(side);
-    cudaStreamDestroy(side);
-  }
   if (stream) cudaStreamDestroy(stream);
-  ev0 = ev1 = evRead = evFork = evJoin = nullptr;
-  stream = side = nullptr;
+  ev0 = ev1 = evRead = nullptr;
+  stream = nullptr;
 }
 
 void* Device::alloc(size_t bytes, const char* what) {

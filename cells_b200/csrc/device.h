@@ -30,9 +30,7 @@ struct Device {
   bool fake = false;
   int ordinal = 0;
   cudaStream_t stream = nullptr;
-  cudaStream_t side = nullptr;  // runs the body kernel beside the bulk kernel
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evRead = nullptr;
-  cudaEvent_t evFork = nullptr, evJoin = nullptr;
   int failAllocAt = 0;  // fake device only: the n-th allocation (1-based) fails
   int nAllocs = 0;
   std::vector<void*> owned;

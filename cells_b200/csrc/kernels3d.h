@@ -47,7 +47,8 @@ struct StepLaunch3 {
   DevState3* st;
   long long N;
   int W, H, D;
-  int bx, by;
+  int tileTX, tileTY;  // interior tile of the step kernel: tileTY rows of tileTX cells
+  int pairTiles;       // 16-bit storage with an even width: two cells per thread
   int nBody;
   int rampKind, rampEvery;
   double rampTarget, rampSteps;
@@ -55,23 +56,14 @@ struct StepLaunch3 {
   int par, sample;
 };
 
-// Streams of one step: the bulk kernel runs on main; the body kernel runs on side (forked from and
-// joined back into main with the two events), or on main after the bulk kernel when side is null.
-struct StepStreams3 {
-  cudaStream_t main;
-  cudaStream_t side;
-  cudaEvent_t fork, join;
-};
-
-// One time step: the bulk kernel and, when there are body cells or the step is sampled, the body
-// kernel. precision: cells_precision (0 f32, 1 f16, 2 bf16, 3 f64). fast: FMA contraction allowed;
-// exact: no contraction, every operation rounds as written.
+// One time step: one launch of the step kernel. precision: cells_precision (0 f32, 1 f16, 2 bf16,
+// 3 f64). fast: FMA contraction allowed; exact: no contraction, every operation rounds as written.
 namespace fast {
-cudaError_t launch_step3(int precision, const StepLaunch3& a, const StepStreams3& ss);
+cudaError_t launch_step3(int precision, const StepLaunch3& a, cudaStream_t s);
 int body_blocks3(int nBody);
 }
 namespace exact {
-cudaError_t launch_step3(int precision, const StepLaunch3& a, const StepStreams3& ss);
+cudaError_t launch_step3(int precision, const StepLaunch3& a, cudaStream_t s);
 int body_blocks3(int nBody);
 }
 

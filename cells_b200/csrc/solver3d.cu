@@ -28,8 +28,8 @@ struct Cells3D {
   long long N = 0;
   int prec = 0;
   size_t bpp = 4;  // bytes per stored population
-  int bx = 32, by = 1;
-  int gx = 1, gy = 1, nBlocks = 1;
+  int bx = 128, by = 1;  // interior tile of the step kernel: by rows of bx cells
+  int pairTiles = 0;     // two cells per thread (16-bit storage, even width)
 
   void* f[2] = {nullptr, nullptr};
   uint32_t* flags = nullptr;
@@ -137,28 +137,28 @@ static void fill_xtab(std::vector<R>& t, int W, double tau, double lambda, doubl
   }
 }
 
+// Interior tile of the step kernel (128 threads per block): 128 cells, or 256 cells as x-pairs for
+// 16-bit storage with an even width. The tile width is workgroup_size when given (the autotuner's
+// knob), else the widest candidate that wastes the fewest threads at the end of a row.
 void Cells3D::choose_launch() {
-  int threads = cfg.workgroup_size > 0 ? cfg.workgroup_size : 256;
-  if (threads > 256) threads = 256;
-  if (threads < 32) threads = 32;
-  threads &= ~31;
+  pairTiles = (bpp == 2 && (W % 2) == 0) ? 1 : 0;
+  const int cells = pairTiles ? 256 : 128;
+  const int lo = pairTiles ? 64 : 32;
   int best = -1;
   long long bestWaste = -1;
-  for (int c = 256; c >= 32; c >>= 1) {
-    if (c > threads) continue;
+  for (int c = cells; c >= lo; c >>= 1) {
     const long long waste = (long long)((W + c - 1) / c) * c - W;
     if (best < 0 || waste < bestWaste) {
       best = c;
       bestWaste = waste;
     }
   }
+  if (cfg.workgroup_size > 0) {
+    best = lo;
+    while (best * 2 <= cells && best * 2 <= cfg.workgroup_size) best *= 2;
+  }
   bx = best;
-  by = threads / bx;
-  while (by > 1 && (H % by) != 0 && ((H + by - 1) / by) * by - H > H / 8) by >>= 1;
-  if (by < 1) by = 1;
-  gx = (W + bx - 1) / bx;
-  gy = (H + by - 1) / by;
-  nBlocks = gx * gy * D;
+  by = cells / bx;
 }
 
 void Cells3D::upload_xtab() {
@@ -245,8 +245,7 @@ void Cells3D::rebuild_flags() {
   argGen++;  // the body list and links are baked into step graphs
 }
 
-// Enqueues the kernels of one step of parity par on `main` (plus the side stream for the body
-// kernel) and returns how many kernels it launched.
+// Enqueues the step kernel of one step of parity par on `main`; returns the kernels launched.
 int Cells3D::enqueue_step(int par, bool sample, cudaStream_t main) {
   StepLaunch3 a;
   a.src = f[par];
@@ -264,8 +263,9 @@ int Cells3D::enqueue_step(int par, bool sample, cudaStream_t main) {
   a.H = H;
   a.D = D;
   a.N = N;
-  a.bx = bx;
-  a.by = by;
+  a.tileTX = bx;
+  a.tileTY = by;
+  a.pairTiles = pairTiles;
   a.nBody = nBody;
   a.rampKind = rampKind;
   a.rampEvery = (int)rampEvery;
@@ -275,10 +275,10 @@ int Cells3D::enqueue_step(int par, bool sample, cudaStream_t main) {
   a.smagC2 = cfg.smagorinsky * cfg.smagorinsky;
   a.par = par;
   a.sample = sample ? 1 : 0;
-  const StepStreams3 ss{main, dev.side, dev.evFork, dev.evJoin};
-  check_cuda(cfg.arithmetic == CELLS_ARITH_EXACT ? exact::launch_step3(prec, a, ss) : fast::launch_step3(prec, a, ss),
-             "step kernels");
-  return (nBody > 0 || sample) ? 2 : 1;
+  check_cuda(cfg.arithmetic == CELLS_ARITH_EXACT ? exact::launch_step3(prec, a, main)
+                                                 : fast::launch_step3(prec, a, main),
+             "step kernel");
+  return 1;
 }
 
 // Steps repeat with period lcm(2, force_every) in their launch arguments (parity and sampling);
@@ -750,7 +750,8 @@ int cells3d_read_params(Cells3D* h, void* out64) {
   u[1] = (uint32_t)h->H;
   u[2] = (uint32_t)h->D;
   u[3] = (uint32_t)h->N;
-  u[4] = (uint32_t)h->gx;
+  // groupsX as the reference derives it for its default workgroup of 128 (src/solver3d.ts:124-127)
+  u[4] = (uint32_t)std::min<long long>((h->N + 127) / 128, 65535);
   f[8] = (float)h->cfg.tau;
   f[9] = (float)h->lambda_value();
   f[10] = (float)(h->cfg.smagorinsky * h->cfg.smagorinsky);

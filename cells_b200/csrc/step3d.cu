@@ -5,21 +5,20 @@
 // Semantics follow the reference kernel src/shaders/step3d.ts:170-223 (main) and :119-168
 // (pullSlow3); the arithmetic order of the moments, equilibria and collision is the generated WGSL's.
 //
-// B200 work split: one time step is two kernels that update disjoint sets of cells, both reading
-// the source buffer and writing the destination buffer.
-//   * bulk3d_kernel: every cell except the body cells. One thread per cell, blocks of (BX x BY)
-//     cells of one z plane, x along warps, so each population load and store of a warp is one
-//     contiguous run of the SoA array f[i*N + cell]. Interior cells take the fast path (19 plain
-//     pulls, no flag read); the inlet plane, the outlet plane and the four slip faces take a
-//     geometric boundary path whose pull sources follow from the coordinates alone. A cell reads
-//     its flag word only when its row (y, z) holds a body cell (rowBody[]); such a cell with a
-//     non-zero flag belongs to the body kernel and is skipped here. No forces arise in this kernel.
-//   * body3d_kernel: the body cells, from a compact list built when the SDF changes: every fluid
-//     cell with a non-zero flag in a row that holds a body cell. It runs the reference's full
-//     pullSlow3 (Bouzidi walls, mirrored sources on solids, momentum exchange) and, on sampled
-//     steps, reduces the forces: warp shuffles in f64, one partial per block, and the last block
-//     to finish sums the partials in a fixed order into the force ring, so the result is
-//     deterministic (the reference sums in atomic slot order, src/shaders/aux3d.ts:80).
+// B200 work split: one launch per time step, its blocks in three roles that update disjoint sets
+// of cells, all reading the source buffer and writing the destination buffer (see step3d_kernel):
+//   * interior rows (y = 1 .. H-2, z = 1 .. D-2): x runs along warps, so each population load and
+//     store of a warp is one contiguous run of the SoA array f[i*N + cell]; the 19 pulls come from
+//     constant-bank bases already shifted by each direction's offset, with no flag read except in
+//     rows that hold a body cell (rowBody[]); the inlet and outlet cells of each row ride along in
+//     the same coalesced loads; 16-bit storage moves two cells per thread;
+//   * the y and z faces: the geometric boundary pull (slip mirrors, edges, outlet copy);
+//   * the body cells (every fluid cell with a flag in a row that holds a body cell): their pulls
+//     (Bouzidi walls, mirrored sources on solids) are resolved into link records when the SDF is
+//     set, so a step reads them with independent loads; on sampled steps the body blocks reduce
+//     the momentum exchange in f64 (warp shuffles, one partial per block, the last block sums the
+//     partials in a fixed order into the force ring), which is deterministic, unlike the
+//     reference's atomic slot order (src/shaders/aux3d.ts:80);
 //   * the relaxation rates and absorbing strength depend on x alone (without Smagorinsky) and come
 //     from a W-entry table that the host fills with the reference's f32 arithmetic.
 #include "kernels3d.h"
@@ -62,6 +61,9 @@ struct StepArgs3 {
   int nBody;
   int rampKind, rampEvery;
   int par, sample;
+  int shellBlocks, bodyBlocks;   // block ranges of the face and body roles
+  int tileTX, tileTY;            // interior tile: tileTY rows of tileTX cells
+  int tilesX, tilesY;
   double rampTarget, rampSteps;
   R lambda, smagC2;
 };
@@ -98,13 +100,18 @@ __device__ __forceinline__ typename C::R feq3s(int i, typename C::R rho, typenam
   return ws3<C>(i) * (rho - R(1) + rho * (cu + R(0.5) * cu * cu - R(1.5) * (ux * ux + uy * uy + uz * uz)));
 }
 
-// Moments, the outlet equilibrium or the TRT collision, and the 19 stores of one cell
-// (src/shaders/step3d.ts:38-102 and :205-223). f holds the pulled populations in storage units;
-// dividing the sums by SCALE and multiplying the weights by SCALE are exact, so every stored value
-// equals the reference formula's.
+// Moments, then the outlet equilibrium or the TRT collision of one cell (src/shaders/step3d.ts:38-102
+// and :205-223), into o. f and o are in storage units; dividing the sums by SCALE and multiplying
+// the weights by SCALE are exact, so every value equals the reference formula's.
+//   * exact arithmetic evaluates the generated WGSL's expressions in its order;
+//   * fast arithmetic evaluates the same TRT update in an equivalent form with about half the
+//     operations per pair: A = omega+ w e - omega+/2 (fa + fb), B = omega- w rho cu - omega-/2 (fa - fb),
+//     fa' = fa + A + B, fb' = fb + A - B, with e = drho + rho (cu^2/2 - 3u^2/2);
+//   * the absorbing layer depends on x alone, so its branch is taken by whole warps (lanes outside
+//     the layer add sources of zero).
 template <class C, bool SMAG>
-__device__ __forceinline__ void collide_store(const StepArgs3<C>& a, const typename C::R (&f)[Q3], int x, int idx,
-                                              bool outlet) {
+__device__ __forceinline__ void collide3(const StepArgs3<C>& a, const typename C::R (&f)[Q3], int x, bool outlet,
+                                         typename C::R (&o)[Q3]) {
   using R = typename C::R;
   constexpr R IS = R(1) / R(C::SCALE);
   // moments, in the generated WGSL's left-to-right order
@@ -121,7 +128,7 @@ __device__ __forceinline__ void collide_store(const StepArgs3<C>& a, const typen
   if (outlet) {
     // pressure outlet: equilibrium at rho = 1 with the node's own velocity
 #pragma unroll
-    for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(feq3s<C>(i, R(1), ux, uy, uz));
+    for (int i = 0; i < Q3; i++) o[i] = feq3s<C>(i, R(1), ux, uy, uz);
     return;
   }
   const auto tab = a.xTab[x];
@@ -159,41 +166,71 @@ __device__ __forceinline__ void collide_store(const StepArgs3<C>& a, const typen
     omM = R(1) / (R(0.5) + a.lambda / (R(1) / omP - R(0.5)));
   }
   // absorbing layer: relax toward the inflow equilibrium
+  const bool absorb = kExact ? sigma > R(0) : __any_sync(__activemask(), sigma > R(0));
   R ut = R(0), dq = R(0);
-  const bool absorb = sigma > R(0);
   if (absorb) {
     ut = (R)a.st->uIn[a.par];
     dq = R(1.5) * rho * (ut * ut - ux * ux - uy * uy - uz * uz);
   }
-  {
-    R s0 = R(0);
-    if (absorb) s0 += sigma * ws3<C>(0) * -dq;
-    R v = f[0] - omP * (f[0] - ws3<C>(0) * (drho - rho * usq));
-    if (kExact || absorb) v = v + s0;
-    a.out[0][idx] = C::enc_raw(v);
-  }
+  if (kExact) {
+    {
+      R s0 = R(0);
+      if (absorb) s0 += sigma * ws3<C>(0) * -dq;
+      o[0] = f[0] - omP * (f[0] - ws3<C>(0) * (drho - rho * usq)) + s0;
+    }
 #pragma unroll
-  for (int p = 1; p < Q3; p += 2) {
-    const R cu = cu_of<R>(p, ux, uy, uz);
-    const R eqS = ws3<C>(p) * (drho + rho * (R(0.5) * cu * cu - usq));
-    const R eqA = ws3<C>(p) * rho * cu;
-    const R sym = omP * (R(0.5) * (f[p] + f[p + 1]) - eqS);
-    const R asym = omM * (R(0.5) * (f[p] - f[p + 1]) - eqA);
-    R va = f[p] - sym - asym;
-    R vb = f[p + 1] - sym + asym;
-    if (kExact || absorb) {
+    for (int p = 1; p < Q3; p += 2) {
+      const R cu = cu_of<R>(p, ux, uy, uz);
+      const R eqS = ws3<C>(p) * (drho + rho * (R(0.5) * cu * cu - usq));
+      const R eqA = ws3<C>(p) * rho * cu;
+      const R sym = omP * (R(0.5) * (f[p] + f[p + 1]) - eqS);
+      const R asym = omM * (R(0.5) * (f[p] - f[p + 1]) - eqA);
       R sS = R(0), sA = R(0);
       if (absorb) {
         const R cut = R(3) * R(cx3(p)) * ut;
         sS += sigma * ws3<C>(p) * (R(0.5) * rho * (cut * cut - cu * cu) - dq);
         sA += sigma * ws3<C>(p) * rho * (cut - cu);
       }
-      va = va + sS + sA;
-      vb = vb + sS - sA;
+      o[p] = f[p] - sym - asym + sS + sA;
+      o[p + 1] = f[p + 1] - sym + asym + sS - sA;
     }
-    a.out[p][idx] = C::enc_raw(va);
-    a.out[p + 1][idx] = C::enc_raw(vb);
+  } else {
+    const R hP = R(0.5) * omP, hM = R(0.5) * omM;
+    const R u3[3] = {R(3) * ux, R(3) * uy, R(3) * uz};
+    const R cP[2] = {omP * ws3<C>(1), omP * ws3<C>(7)};
+    const R cM[2] = {omM * ws3<C>(1) * rho, omM * ws3<C>(7) * rho};
+    R v0 = f[0] - omP * (f[0] - ws3<C>(0) * (drho - rho * usq));
+    if (absorb) v0 += sigma * ws3<C>(0) * -dq;
+    o[0] = v0;
+#pragma unroll
+    for (int p = 1; p < Q3; p += 2) {
+      const int k = p <= 5 ? 0 : 1;
+      R cu = R(0);
+      if (cx3(p)) cu += R(cx3(p)) * u3[0];
+      if (cy3(p)) cu += R(cy3(p)) * u3[1];
+      if (cz3(p)) cu += R(cz3(p)) * u3[2];
+      const R e = rho * (cu * (R(0.5) * cu) - usq) + drho;
+      R A = cP[k] * e - hP * (f[p] + f[p + 1]);
+      R B = cM[k] * cu - hM * (f[p] - f[p + 1]);
+      if (absorb) {
+        const R cut = R(3) * R(cx3(p)) * ut;
+        const R sw = sigma * ws3<C>(p);
+        A += sw * (R(0.5) * rho * (cut * cut - cu * cu) - dq);
+        B += sw * rho * (cut - cu);
+      }
+      o[p] = f[p] + A + B;
+      o[p + 1] = f[p + 1] + A - B;
+    }
   }
+}
+
+template <class C, bool SMAG>
+__device__ __forceinline__ void collide_store(const StepArgs3<C>& a, const typename C::R (&f)[Q3], int x, int idx,
+                                              bool outlet) {
+  typename C::R o[Q3];
+  collide3<C, SMAG>(a, f, x, outlet, o);
+#pragma unroll
+  for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(o[i]);
 }
 
 __device__ __forceinline__ double ramp_speed(int kind, double target, double rampSteps, int every, unsigned step) {
@@ -202,89 +239,111 @@ __device__ __forceinline__ double ramp_speed(int kind, double target, double ram
   return kind == 1 ? target * t : target * (t * t * (3.0 - 2.0 * t));
 }
 
-// ---------------- bulk kernel ----------------
+// ---------------- the step kernel: one launch per time step ----------------
+//
+// Blocks of 128 threads take one of three roles by block index (computed on the host):
+//   [0, shellBlocks)                      the face cells: z = 0 and z = D-1 planes, y = 0 and y = H-1
+//                                         rows of the planes between, one cell per thread, x fastest;
+//   [shellBlocks, + bodyBlocks)           32 body cells per block, their 19 links resolved in parallel;
+//   [shellBlocks + bodyBlocks, + tiles)   the rows y = 1 .. H-2 of planes z = 1 .. D-2 in tiles of
+//                                         tileTY rows of tileTX cells (two cells per thread for
+//                                         16-bit storage, one otherwise).
+// The face and body blocks have the lowest indices, so they are dispatched first and run beside
+// the first interior tiles. Cells a role does not own it leaves alone: in a row that holds a body
+// cell, every cell with a flag belongs to the body role. Block 0 also advances the device step
+// counter and the device-side inlet ramp for the next step.
 
+constexpr int kStepThreads = 128;
+
+// Number of cells on the faces: the z = 0 and z = D-1 planes and the y = 0 and y = H-1 rows of the
+// planes between.
+__host__ __device__ __forceinline__ long long shell_cells3(int W, int H, int D) {
+  const long long nz = D >= 2 ? 2 : 1, ny = H >= 2 ? 2 : 1;
+  const long long inD = D > 2 ? D - 2 : 0;
+  return nz * W * H + ny * W * inD;
+}
+
+// A face cell: pullSlow3 (step3d.ts:119-168) for a cell without solid neighbours, every mirrored
+// source being fluid; the inlet cell stores the inflow equilibrium.
 template <class C, bool SMAG>
-__global__ void __launch_bounds__(256, sizeof(typename C::R) == 8 ? 2 : 4)
-    bulk3d_kernel(const __grid_constant__ StepArgs3<C> a) {
+__device__ __forceinline__ void shell_role(const StepArgs3<C>& a, int b) {
   using R = typename C::R;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
-    const unsigned s = a.st->step[a.par];
-    a.st->step[a.par ^ 1] = s + 1u;
-    if (a.rampKind != 0)
-      a.st->uIn[a.par ^ 1] = ramp_speed(a.rampKind, a.rampTarget, a.rampSteps, a.rampEvery, s + 1u);
-  }
   const int W = a.W, H = a.H, D = a.D;
-  if (x >= W || y >= H) return;
+  long long t = (long long)b * kStepThreads + threadIdx.x;
+  int x, y, z;
+  const long long nzp = D >= 2 ? 2 : 1, nyr = H >= 2 ? 2 : 1;
+  const long long inD = D > 2 ? D - 2 : 0;
+  const long long cz = nzp * W * H, cy = nyr * W * inD;
+  if (t < cz) {
+    const long long plane = t / ((long long)W * H);
+    const long long r = t - plane * W * H;
+    z = plane == 0 ? 0 : D - 1;
+    y = (int)(r / W);
+    x = (int)(r - (long long)y * W);
+  } else if ((t -= cz) < cy) {
+    const long long side = t / (W * inD);
+    const long long r = t - side * W * inD;
+    y = side == 0 ? 0 : H - 1;
+    z = 1 + (int)(r / W);
+    x = (int)(r - (long long)(z - 1) * W);
+  } else {
+    return;
+  }
   const int row = y + H * z;
   const int idx = x + W * row;
-  const bool interior = x > 0 && x < W - 1 && y > 0 && y < H - 1 && z > 0 && z < D - 1;
-  if (a.rowBody[row]) {
-    // rows holding a body cell: any cell with a flag belongs to the body kernel
-    if (__ldg(a.flags + idx) != 0u) return;
+  if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
+  if (x == 0) {
+    // inlet: equilibrium at the inflow speed, no collision (step3d.ts:190-193)
+    const R u = (R)a.st->uIn[a.par];
+#pragma unroll
+    for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(feq3s<C>(i, R(1), u, R(0), R(0)));
+    return;
   }
+  const bool outlet = x == W - 1;
+  const long long N = a.N;
+  const long long WH = (long long)W * H;
   R f[Q3];
-  bool outlet = false;
-  if (interior) {
+  f[0] = C::raw(a.src + idx);
 #pragma unroll
-    for (int i = 0; i < Q3; i++) f[i] = C::raw(a.pull[i] + idx);
-  } else {
-    if (x == 0) {
-      // inlet: equilibrium at the inflow speed, no collision (step3d.ts:190-193)
-      const R u = (R)a.st->uIn[a.par];
-#pragma unroll
-      for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(feq3s<C>(i, R(1), u, R(0), R(0)));
-      return;
+  for (int i = 1; i < Q3; i++) {
+    const int sx = x - cx3(i), sy = y - cy3(i), sz = z - cz3(i);
+    const bool outX = sx < 0 || sx >= W;
+    const bool outY = sy < 0 || sy >= H;
+    const bool outZ = sz < 0 || sz >= D;
+    int pop = i;
+    long long cell;
+    if (!(outX || outY || outZ)) {
+      cell = idx - (cx3(i) + cy3(i) * (long long)W + cz3(i) * WH);
+    } else if (outX && outlet) {
+      cell = (long long)(W - 2) + (long long)W * row;  // outlet: zero-gradient copy
+    } else if (outY && outZ) {
+      pop = opp3(i);  // edge: the double mirror equals bounce-back
+      cell = idx;
+    } else if (outY || outZ) {
+      pop = outY ? mirror_y3(i) : mirror_z3(i);  // slip: specular reflection
+      const int ry = outY ? y : sy;
+      const int rz = outY ? sz : z;
+      cell = (long long)sx + (long long)W * (ry + (long long)H * rz);
+    } else {
+      pop = opp3(i);
+      cell = idx;
     }
-    outlet = x == W - 1;
-    // geometric boundary pull: pullSlow3 (step3d.ts:119-168) for a cell without solid neighbours,
-    // so every mirrored source is fluid
-    const long long N = a.N;
-    const long long WH = (long long)W * H;
-    f[0] = C::raw(a.src + idx);
-#pragma unroll
-    for (int i = 1; i < Q3; i++) {
-      const int sx = x - cx3(i), sy = y - cy3(i), sz = z - cz3(i);
-      const bool outX = sx < 0 || sx >= W;
-      const bool outY = sy < 0 || sy >= H;
-      const bool outZ = sz < 0 || sz >= D;
-      int pop = i;
-      long long cell;
-      if (!(outX || outY || outZ)) {
-        cell = idx - (cx3(i) + cy3(i) * (long long)W + cz3(i) * WH);
-      } else if (outX && outlet) {
-        cell = (long long)(W - 2) + (long long)W * row;  // outlet: zero-gradient copy
-      } else if (outY && outZ) {
-        pop = opp3(i);  // edge: the double mirror equals bounce-back
-        cell = idx;
-      } else if (outY || outZ) {
-        pop = outY ? mirror_y3(i) : mirror_z3(i);  // slip: specular reflection
-        const int ry = outY ? y : sy;
-        const int rz = outY ? sz : z;
-        cell = (long long)sx + (long long)W * (ry + (long long)H * rz);
-      } else {
-        pop = opp3(i);
-        cell = idx;
-      }
-      f[i] = C::raw(a.src + (long long)pop * N + cell);
-    }
+    f[i] = C::raw(a.src + (long long)pop * N + cell);
   }
   collide_store<C, SMAG>(a, f, x, idx, outlet);
 }
 
-// ---------------- body kernel ----------------
-
+// Sum of the block's forces in f64 (warp shuffles, then the warps in order) into partials[slot];
+// the last of the nSlots body blocks to finish sums the partials in slot order into the force
+// ring. Deterministic for a fixed body list.
 template <class C>
-__device__ __forceinline__ void finish_forces(typename C::R fx, typename C::R fy, typename C::R fz, int nSlots,
-                                              double4* __restrict__ partials, double4* __restrict__ history,
-                                              DevState3* __restrict__ st) {
-  __shared__ double red[3][32];
+__device__ __forceinline__ void finish_forces(typename C::R fx, typename C::R fy, typename C::R fz, int slot,
+                                              int nSlots, double4* __restrict__ partials,
+                                              double4* __restrict__ history, DevState3* __restrict__ st) {
+  __shared__ double red[3][kStepThreads / 32];
   __shared__ int amLast;
-  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-  const int lane = tid & 31, warp = tid >> 5, nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
   double dx = (double)fx, dy = (double)fy, dz = (double)fz;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -300,12 +359,12 @@ __device__ __forceinline__ void finish_forces(typename C::R fx, typename C::R fy
   __syncthreads();
   if (tid == 0) {
     double sx = 0.0, sy = 0.0, sz = 0.0;
-    for (int w = 0; w < nwarps; w++) {
+    for (int w = 0; w < kStepThreads / 32; w++) {
       sx += red[0][w];
       sy += red[1][w];
       sz += red[2][w];
     }
-    partials[blockIdx.x] = make_double4(sx, sy, sz, 0.0);
+    partials[slot] = make_double4(sx, sy, sz, 0.0);
     __threadfence();
     const unsigned prev = atomicAdd(&st->done, 1u);
     amLast = (prev == (unsigned)(nSlots - 1));
@@ -338,42 +397,43 @@ __device__ __forceinline__ void finish_forces(typename C::R fx, typename C::R fy
   }
 }
 
-// One block handles 32 body cells with 32 x 19 threads: thread (lane, i) resolves link i of cell
-// lane (a record load, then one or two source loads, all independent across threads) into shared
-// memory; then one thread per cell sums the momentum exchange in the reference's direction order
-// and collides.
+// 32 body cells: item (lane, i) resolves link i of cell lane (a record load, then one or two
+// source loads, independent across items) into shared memory; then one thread per cell sums the
+// momentum exchange in the reference's direction order and collides.
 template <class C, bool SMAG>
-__global__ void __launch_bounds__(32 * Q3) body3d_kernel(const __grid_constant__ StepArgs3<C> a) {
+__device__ __forceinline__ void body_role(const StepArgs3<C>& a, int bb) {
   using R = typename C::R;
   __shared__ R sv[Q3][32];  // pulled populations in storage units
   __shared__ R sm[Q3][32];  // momentum-exchange term of each link (0 when the link exchanges none)
-  const int lane = threadIdx.x, dir = threadIdx.y;
-  const int t = blockIdx.x * 32 + lane;
-  const bool valid = t < a.nBody;
-  if (valid) {
+  for (int item = threadIdx.x; item < 32 * Q3; item += kStepThreads) {
+    const int lane = item & 31, dir = item >> 5;
+    const int t = bb * 32 + lane;
+    if (t >= a.nBody) continue;
     const int idx = a.bodyCells[t];
     if (dir == 0) {
       sv[0][lane] = C::raw(a.src + idx);
-    } else {
-      const int kind = (int)((__ldg(a.links.kinds + t) >> (3 * (dir - 1))) & 7ull);
-      const Link3<R> L = ((const Link3<R>*)a.links.rec)[(long long)(dir - 1) * a.links.cap + t];
-      const R fj = C::raw(a.src + L.e1);
-      R v = fj, m = R(0);
-      if (kind == LINK_SLIP_SOLID) {
-        m = R(2) * fj;  // a body meets the slip face: bounce-back
-      } else if (kind >= LINK_BOUZIDI_N) {
-        // Bouzidi linear interpolated bounce-back (step3d.ts:152-167)
-        if (kind == LINK_BOUZIDI_N) v = L.c1 * fj + L.c2 * C::raw(a.src + L.e2);
-        else if (kind == LINK_BOUZIDI_H) v = fj / L.c1 + L.c2 * C::raw(a.src + L.e2);
-        m = fj + v;
-      }
-      sv[dir][lane] = v;
-      sm[dir][lane] = m;
+      continue;
     }
+    const int kind = (int)((__ldg(a.links.kinds + t) >> (3 * (dir - 1))) & 7ull);
+    const Link3<R> L = ((const Link3<R>*)a.links.rec)[(long long)(dir - 1) * a.links.cap + t];
+    const R fj = C::raw(a.src + L.e1);
+    R v = fj, m = R(0);
+    if (kind == LINK_SLIP_SOLID) {
+      m = R(2) * fj;  // a body meets the slip face: bounce-back
+    } else if (kind >= LINK_BOUZIDI_N) {
+      // Bouzidi linear interpolated bounce-back (step3d.ts:152-167)
+      if (kind == LINK_BOUZIDI_N) v = L.c1 * fj + L.c2 * C::raw(a.src + L.e2);
+      else if (kind == LINK_BOUZIDI_H) v = fj / L.c1 + L.c2 * C::raw(a.src + L.e2);
+      m = fj + v;
+    }
+    sv[dir][lane] = v;
+    sm[dir][lane] = m;
   }
   __syncthreads();
   R fx = R(0), fy = R(0), fz = R(0);
-  if (dir == 0 && valid) do {
+  const int lane = threadIdx.x;
+  const int t = bb * 32 + lane;
+  if (lane < 32 && t < a.nBody) do {
       const int idx = a.bodyCells[t];
       const int meta = a.links.meta[t];
       const int x = meta & ((1 << 29) - 1);
@@ -401,15 +461,163 @@ __global__ void __launch_bounds__(32 * Q3) body3d_kernel(const __grid_constant__
     } while (0);
   // the momentum exchange was summed in storage units
   constexpr R IS = R(1) / R(C::SCALE);
-  if (a.sample) finish_forces<C>(fx * IS, fy * IS, fz * IS, (int)gridDim.x, a.partials, a.history, a.st);
+  if (a.sample) finish_forces<C>(fx * IS, fy * IS, fz * IS, bb, a.bodyBlocks, a.partials, a.history, a.st);
+}
+
+// Interior rows, one cell per thread. Interior cells pull their 19 populations from the
+// constant-bank shifted bases. The outlet cell (x = W-1) pulls the same way except for the five
+// directions with c_x = -1, whose source is the copy from (W-2, y, z): a fixed index offset per
+// direction, so all lanes of a warp still issue the same coalesced loads. The inlet cell (x = 0)
+// loads nothing and stores the inflow equilibrium; inlet and outlet stores are short tails, paid
+// once per row.
+template <class C, bool SMAG>
+__device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int k) {
+  using R = typename C::R;
+  const int tx = k % a.tilesX;
+  const int ty = (k / a.tilesX) % a.tilesY;
+  const int tz = k / (a.tilesX * a.tilesY);
+  const int lx = threadIdx.x % a.tileTX, ly = threadIdx.x / a.tileTX;
+  const int x = tx * a.tileTX + lx;
+  const int y = 1 + ty * a.tileTY + ly;
+  const int z = 1 + tz;
+  const int W = a.W, H = a.H;
+  if (x >= W || y >= H - 1) return;
+  const int row = y + H * z;
+  const int idx = x + W * row;
+  if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
+  if (x == 0) {
+    // inlet: equilibrium at the inflow speed, no collision (step3d.ts:190-193)
+    const R u = (R)a.st->uIn[a.par];
+#pragma unroll
+    for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(feq3s<C>(i, R(1), u, R(0), R(0)));
+    return;
+  }
+  const bool outlet = x == W - 1;
+  const long long WH = (long long)W * H;
+  R f[Q3];
+#pragma unroll
+  for (int i = 0; i < Q3; i++) {
+    int e = idx;
+    // outlet: zero-gradient copy from (W-2, y, z) for the directions entering through x = W-1
+    if (cx3(i) == -1 && outlet) e += (int)(-2 + cy3(i) * (long long)W + cz3(i) * WH);
+    f[i] = C::raw(a.pull[i] + e);
+  }
+  collide_store<C, SMAG>(a, f, x, idx, outlet);
+}
+
+// Interior rows for 16-bit storage (f16, bf16) and an even width: each thread updates the x-pair
+// (x0, x0 + 1), x0 even. One address per population serves both cells; the populations with c_x = 0
+// arrive as one 32-bit load (both cells' values), the others as two 16-bit loads; the 19 results are
+// rounded as a pair and stored with one 32-bit store. Cells of the pair that belong to the body role
+// are left alone.
+template <class C, bool SMAG>
+__device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int k) {
+  using R = typename C::R;
+  using S = typename C::S;
+  const int tx = k % a.tilesX;
+  const int ty = (k / a.tilesX) % a.tilesY;
+  const int tz = k / (a.tilesX * a.tilesY);
+  const int tpr = a.tileTX / 2;  // threads per tile row
+  const int lx = threadIdx.x % tpr, ly = threadIdx.x / tpr;
+  const int x0 = tx * a.tileTX + 2 * lx;
+  const int y = 1 + ty * a.tileTY + ly;
+  const int z = 1 + tz;
+  const int W = a.W, H = a.H;
+  if (x0 >= W || y >= H - 1) return;
+  const int row = y + H * z;
+  const int idx = x0 + W * row;
+  bool act0 = true, act1 = true;
+  if (a.rowBody[row]) {
+    act0 = __ldg(a.flags + idx) == 0u;
+    act1 = __ldg(a.flags + idx + 1) == 0u;
+    if (!act0 && !act1) return;
+  }
+  const bool inlet0 = x0 == 0;
+  const bool outlet1 = x0 + 1 == W - 1;
+  const long long WH = (long long)W * H;
+  uint32_t r[Q3];  // populations of the pair: x0 in the low half, x0 + 1 in the high half
+#pragma unroll
+  for (int i = 0; i < Q3; i++) {
+    const S* p = a.pull[i] + idx;
+    if (cx3(i) == 0) {
+      r[i] = __ldg(reinterpret_cast<const unsigned int*>(p));
+    } else {
+      int e1 = 1;
+      // outlet: zero-gradient copy from (W-2, y, z) for the directions entering through x = W-1
+      if (cx3(i) == -1 && outlet1) e1 += (int)(-2 + cy3(i) * (long long)W + cz3(i) * WH);
+      const uint32_t v0 = __ldg(reinterpret_cast<const unsigned short*>(p));
+      const uint32_t v1 = __ldg(reinterpret_cast<const unsigned short*>(p + e1));
+      r[i] = v0 | (v1 << 16);
+    }
+  }
+  R o0[Q3];
+  if (act0) {
+    if (inlet0) {
+      // inlet: equilibrium at the inflow speed, no collision (step3d.ts:190-193)
+      const R u = (R)a.st->uIn[a.par];
+#pragma unroll
+      for (int i = 0; i < Q3; i++) o0[i] = feq3s<C>(i, R(1), u, R(0), R(0));
+    } else {
+      R f[Q3];
+#pragma unroll
+      for (int i = 0; i < Q3; i++) f[i] = C::lo(r[i]);
+      collide3<C, SMAG>(a, f, x0, false, o0);
+    }
+  }
+  R o1[Q3];
+  if (act1) {
+    R f[Q3];
+#pragma unroll
+    for (int i = 0; i < Q3; i++) f[i] = C::hi(r[i]);
+    collide3<C, SMAG>(a, f, x0 + 1, outlet1, o1);
+  }
+  if (act0 && act1) {
+#pragma unroll
+    for (int i = 0; i < Q3; i++) *reinterpret_cast<uint32_t*>(a.out[i] + idx) = C::pack2(o0[i], o1[i]);
+  } else if (act0) {
+#pragma unroll
+    for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(o0[i]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < Q3; i++) a.out[i][idx + 1] = C::enc_raw(o1[i]);
+  }
+}
+
+template <class C>
+constexpr int step_min_blocks(bool pair) {
+  return pair ? 6 : (sizeof(typename C::R) == 8 ? 4 : 8);
+}
+
+template <class C, bool SMAG, bool PAIR>
+__global__ void __launch_bounds__(kStepThreads, step_min_blocks<C>(PAIR))
+    step3d_kernel(const __grid_constant__ StepArgs3<C> a) {
+  int b = blockIdx.x;
+  if (b == 0 && threadIdx.x == 0) {
+    const unsigned s = a.st->step[a.par];
+    a.st->step[a.par ^ 1] = s + 1u;
+    if (a.rampKind != 0)
+      a.st->uIn[a.par ^ 1] = ramp_speed(a.rampKind, a.rampTarget, a.rampSteps, a.rampEvery, s + 1u);
+  }
+  if (b < a.shellBlocks) {
+    shell_role<C, SMAG>(a, b);
+    return;
+  }
+  b -= a.shellBlocks;
+  if (b < a.bodyBlocks) {
+    body_role<C, SMAG>(a, b);
+    return;
+  }
+  b -= a.bodyBlocks;
+  if constexpr (PAIR)
+    bulk_pair_role<C, SMAG>(a, b);
+  else
+    bulk_role<C, SMAG>(a, b);
 }
 
 // ---------------- host-side launcher ----------------
 
-int body_blocks3(int nBody);
-
 template <class C>
-static cudaError_t launch_step3_t(const StepLaunch3& L, const StepStreams3& ss) {
+static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   using R = typename C::R;
   using S = typename C::S;
   StepArgs3<C> a;
@@ -443,45 +651,42 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, const StepStreams3& ss) 
   a.rampSteps = L.rampSteps;
   a.lambda = (R)L.lambda;
   a.smagC2 = (R)L.smagC2;
-  dim3 block(L.bx, L.by, 1);
-  dim3 grid((L.W + L.bx - 1) / L.bx, (L.H + L.by - 1) / L.by, L.D);
+  // work split
+  const long long nShell = shell_cells3(L.W, L.H, L.D);
+  a.shellBlocks = (int)((nShell + kStepThreads - 1) / kStepThreads);
+  // the body role runs when there are body cells, and on sampled steps even without them (a
+  // sample of zero force is still written to the ring, as the reference's reduce pass does)
+  a.bodyBlocks = (L.nBody > 0 || L.sample) ? body_blocks3(L.nBody) : 0;
+  const bool pair = sizeof(S) == 2 && (L.W % 2) == 0 && L.tileTX >= 64 && L.pairTiles;
+  a.tileTX = L.tileTX;
+  a.tileTY = L.tileTY;
+  a.tilesX = (L.W + L.tileTX - 1) / L.tileTX;
+  a.tilesY = L.H > 2 ? (L.H - 2 + L.tileTY - 1) / L.tileTY : 0;
+  const long long tiles = (L.H > 2 && L.D > 2) ? (long long)a.tilesX * a.tilesY * (L.D - 2) : 0;
+  const long long blocks = (long long)a.shellBlocks + a.bodyBlocks + tiles;
   const bool smag = L.smagC2 > 0;
-  cudaError_t e;
-  // the body kernel runs when there are body cells, and on sampled steps even without them (a
-  // sample of zero force is still written to the ring, as the reference's reduce pass does). The
-  // two kernels touch disjoint cells, so the body kernel runs on a side stream beside the bulk one.
-  const bool body = L.nBody > 0 || L.sample;
-  const bool side = body && ss.side != nullptr;
-  cudaStream_t bs = side ? ss.side : ss.main;
-  if (side) {
-    if ((e = cudaEventRecord(ss.fork, ss.main)) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(ss.side, ss.fork, 0)) != cudaSuccess) return e;
-  }
-  if (body) {
-    const int blocks = body_blocks3(L.nBody);
-    const dim3 bblock(32, Q3, 1);
+  if (pair) {
+    if constexpr (sizeof(S) == 2) {
+      if (smag)
+        step3d_kernel<C, true, true><<<(unsigned)blocks, kStepThreads, 0, s>>>(a);
+      else
+        step3d_kernel<C, false, true><<<(unsigned)blocks, kStepThreads, 0, s>>>(a);
+    }
+  } else {
     if (smag)
-      body3d_kernel<C, true><<<blocks, bblock, 0, bs>>>(a);
+      step3d_kernel<C, true, false><<<(unsigned)blocks, kStepThreads, 0, s>>>(a);
     else
-      body3d_kernel<C, false><<<blocks, bblock, 0, bs>>>(a);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      step3d_kernel<C, false, false><<<(unsigned)blocks, kStepThreads, 0, s>>>(a);
   }
-  if (side && (e = cudaEventRecord(ss.join, ss.side)) != cudaSuccess) return e;
-  if (smag)
-    bulk3d_kernel<C, true><<<grid, block, 0, ss.main>>>(a);
-  else
-    bulk3d_kernel<C, false><<<grid, block, 0, ss.main>>>(a);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if (side) e = cudaStreamWaitEvent(ss.main, ss.join, 0);
-  return e;
+  return cudaGetLastError();
 }
 
-cudaError_t launch_step3(int precision, const StepLaunch3& a, const StepStreams3& ss) {
+cudaError_t launch_step3(int precision, const StepLaunch3& a, cudaStream_t s) {
   switch (precision) {
-    case 0: return launch_step3_t<CodecF32>(a, ss);
-    case 1: return launch_step3_t<CodecF16>(a, ss);
-    case 2: return launch_step3_t<CodecBF16>(a, ss);
-    case 3: return launch_step3_t<CodecF64>(a, ss);
+    case 0: return launch_step3_t<CodecF32>(a, s);
+    case 1: return launch_step3_t<CodecF16>(a, s);
+    case 2: return launch_step3_t<CodecBF16>(a, s);
+    case 3: return launch_step3_t<CodecF64>(a, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -213,5 +213,5 @@ def test_graph_replay_matches_oracle(every):
     o.encodeSteps(200)
     assert_same(s, o, True)
     assert_forces(s.readForces(), o.readForces(), 1e-9)
-    assert s.launchCount() > 2 * 596  # every step launched the bulk kernel and most the body kernel
+    assert s.launchCount() >= 596  # one step kernel per step, whether replayed from a graph or not
     s.destroy()

@@ -282,7 +282,9 @@ __global__ void sum_partials_kernel(const double* __restrict__ partials, int n, 
 
 // which: bit 0 writes the step counters, bit 1 the inlet speeds, bit 2 clears the sample counter,
 // bit 3 clears the status word.
+template <class C>
 __global__ void set_state3_kernel(DevState3* st, int which, unsigned step, double u0, double u1) {
+  using R = typename C::R;
   if (which & 1) {
     st->step[0] = step;
     st->step[1] = step;
@@ -290,6 +292,12 @@ __global__ void set_state3_kernel(DevState3* st, int which, unsigned step, doubl
   if (which & 2) {
     st->uIn[0] = u0;
     st->uIn[1] = u1;
+    // inlet equilibrium in storage units, as the step kernels compute it (src/shaders/common3d.ts:38-41)
+    for (int k = 0; k < 2; k++) {
+      const R u = (R)(k == 0 ? u0 : u1);
+      for (int i = 0; i < Q3; i++)
+        st->inletEq[k][i] = (double)(feq3a<R>(i, R(1), u, R(0), R(0)) * R(C::SCALE));
+    }
   }
   if (which & 4) {
     st->sample = 0u;
@@ -345,8 +353,9 @@ cudaError_t launch_mass3(int precision, const AuxLaunch3& a, const void* f, cons
   return cudaGetLastError();
 }
 
-cudaError_t launch_set_state3(DevState3* st, int which, unsigned step, double uIn0, double uIn1, cudaStream_t s) {
-  set_state3_kernel<<<1, 1, 0, s>>>(st, which, step, uIn0, uIn1);
+cudaError_t launch_set_state3(int precision, DevState3* st, int which, unsigned step, double uIn0, double uIn1,
+                              cudaStream_t s) {
+  CELLS_DISPATCH(precision, (set_state3_kernel<C><<<1, 1, 0, s>>>(st, which, step, uIn0, uIn1)));
   return cudaGetLastError();
 }
 

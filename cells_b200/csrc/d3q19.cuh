@@ -134,6 +134,9 @@ struct DevState3 {
   unsigned int status;  // bit 0: non-finite force sample, bit 1: non-finite macro value
   unsigned int pad[3];
   double uIn[2];
+  // the inlet's 19 equilibrium values feq(i, 1, uIn, 0, 0) in storage units, per parity slot (they
+  // depend on uIn alone, so a step reads them instead of every inlet cell computing them)
+  double inletEq[2][Q3];
 };
 
 // Launch-invariant parameters of a step (kernel arguments). The x-dependent relaxation rate and

@@ -91,6 +91,7 @@ cudaError_t launch_mass3(int precision, const AuxLaunch3& a, const void* f, cons
                          int nPartials, double* out, cudaStream_t s);
 // Writes parts of the device state in stream order. which: bit 0 both step counters, bit 1 both
 // inlet speeds, bit 2 clears the force sample counter, bit 3 clears the status word.
-cudaError_t launch_set_state3(DevState3* st, int which, unsigned step, double uIn0, double uIn1, cudaStream_t s);
+cudaError_t launch_set_state3(int precision, DevState3* st, int which, unsigned step, double uIn0, double uIn1,
+                              cudaStream_t s);
 
 }  // namespace cells

@@ -184,7 +184,7 @@ void Cells3D::write_state(int which) {
     return;
   }
   const double u = current_uin();
-  check_cuda(launch_set_state3(st, which, (unsigned)step, u, u, dev.stream), "set_state kernel");
+  check_cuda(launch_set_state3(prec, st, which, (unsigned)step, u, u, dev.stream), "set_state kernel");
   dev.launches++;
 }
 

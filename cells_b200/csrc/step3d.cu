@@ -63,7 +63,7 @@ struct StepArgs3 {
   int par, sample;
   int shellBlocks, bodyBlocks;   // block ranges of the face and body roles
   int tileTX, tileTY;            // interior tile: tileTY rows of tileTX cells
-  int tilesX, tilesY;
+  int roleZ;                     // grid z-slices holding the face and body roles
   double rampTarget, rampSteps;
   R lambda, smagC2;
 };
@@ -120,15 +120,32 @@ __device__ __forceinline__ void collide3(const StepArgs3<C>& a, const typename C
   for (int i = 1; i < Q3; i++) dsum = dsum + f[i];
   const R drho = dsum * IS;
   const R rho = R(1) + drho;
-  const R invRho = R(1) / rho;
+  // fast arithmetic: the hardware reciprocal (branch-free, within 2 ulp) instead of IEEE division
+  R invRho;
+  if constexpr (!kExact && sizeof(R) == 4)
+    invRho = __fdividef(R(1), rho);
+  else
+    invRho = R(1) / rho;
   const R ux = ((f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[13] - f[14] + f[15] - f[16]) * IS) * invRho;
   const R uy = ((f[3] - f[4] + f[7] - f[8] + f[11] - f[12] - f[13] + f[14] + f[17] - f[18]) * IS) * invRho;
   const R uz = ((f[5] - f[6] + f[9] - f[10] + f[11] - f[12] - f[15] + f[16] - f[17] + f[18]) * IS) * invRho;
   const R usq = R(1.5) * (ux * ux + uy * uy + uz * uz);
   if (outlet) {
-    // pressure outlet: equilibrium at rho = 1 with the node's own velocity
+    // pressure outlet: equilibrium at rho = 1 with the node's own velocity; fast arithmetic uses
+    // feq_a,b = w (t +- cu) with t = cu^2/2 - 3u^2/2, sharing t between the pair
+    if (kExact) {
 #pragma unroll
-    for (int i = 0; i < Q3; i++) o[i] = feq3s<C>(i, R(1), ux, uy, uz);
+      for (int i = 0; i < Q3; i++) o[i] = feq3s<C>(i, R(1), ux, uy, uz);
+    } else {
+      o[0] = -ws3<C>(0) * usq;
+#pragma unroll
+      for (int p = 1; p < Q3; p += 2) {
+        const R cu = cu_of<R>(p, ux, uy, uz);
+        const R t = cu * (R(0.5) * cu) - usq;
+        o[p] = ws3<C>(p) * (t + cu);
+        o[p + 1] = ws3<C>(p) * (t - cu);
+      }
+    }
     return;
   }
   const auto tab = a.xTab[x];
@@ -205,10 +222,18 @@ __device__ __forceinline__ void collide3(const StepArgs3<C>& a, const typename C
 #pragma unroll
     for (int p = 1; p < Q3; p += 2) {
       const int k = p <= 5 ? 0 : 1;
-      R cu = R(0);
-      if (cx3(p)) cu += R(cx3(p)) * u3[0];
-      if (cy3(p)) cu += R(cy3(p)) * u3[1];
-      if (cz3(p)) cu += R(cz3(p)) * u3[2];
+      R cu;
+      switch (p) {  // 3 (c_p . u) from the precomputed 3u
+        case 1: cu = u3[0]; break;
+        case 3: cu = u3[1]; break;
+        case 5: cu = u3[2]; break;
+        case 7: cu = u3[0] + u3[1]; break;
+        case 9: cu = u3[0] + u3[2]; break;
+        case 11: cu = u3[1] + u3[2]; break;
+        case 13: cu = u3[0] - u3[1]; break;
+        case 15: cu = u3[0] - u3[2]; break;
+        default: cu = u3[1] - u3[2]; break;
+      }
       const R e = rho * (cu * (R(0.5) * cu) - usq) + drho;
       R A = cP[k] * e - hP * (f[p] + f[p + 1]);
       R B = cM[k] * cu - hM * (f[p] - f[p + 1]);
@@ -266,10 +291,10 @@ __host__ __device__ __forceinline__ long long shell_cells3(int W, int H, int D) 
 // A face cell: pullSlow3 (step3d.ts:119-168) for a cell without solid neighbours, every mirrored
 // source being fluid; the inlet cell stores the inflow equilibrium.
 template <class C, bool SMAG>
-__device__ __forceinline__ void shell_role(const StepArgs3<C>& a, int b) {
+__device__ __forceinline__ void shell_role(const StepArgs3<C>& a, int b, int tid) {
   using R = typename C::R;
   const int W = a.W, H = a.H, D = a.D;
-  long long t = (long long)b * kStepThreads + threadIdx.x;
+  long long t = (long long)b * kStepThreads + tid;
   int x, y, z;
   const long long nzp = D >= 2 ? 2 : 1, nyr = H >= 2 ? 2 : 1;
   const long long inD = D > 2 ? D - 2 : 0;
@@ -294,9 +319,9 @@ __device__ __forceinline__ void shell_role(const StepArgs3<C>& a, int b) {
   if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
   if (x == 0) {
     // inlet: equilibrium at the inflow speed, no collision (step3d.ts:190-193)
-    const R u = (R)a.st->uIn[a.par];
+    const double* eq = a.st->inletEq[a.par];
 #pragma unroll
-    for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(feq3s<C>(i, R(1), u, R(0), R(0)));
+    for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw((R)eq[i]);
     return;
   }
   const bool outlet = x == W - 1;
@@ -339,10 +364,9 @@ __device__ __forceinline__ void shell_role(const StepArgs3<C>& a, int b) {
 template <class C>
 __device__ __forceinline__ void finish_forces(typename C::R fx, typename C::R fy, typename C::R fz, int slot,
                                               int nSlots, double4* __restrict__ partials,
-                                              double4* __restrict__ history, DevState3* __restrict__ st) {
+                                              double4* __restrict__ history, DevState3* __restrict__ st, int tid) {
   __shared__ double red[3][kStepThreads / 32];
   __shared__ int amLast;
-  const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   double dx = (double)fx, dy = (double)fy, dz = (double)fz;
 #pragma unroll
@@ -401,11 +425,11 @@ __device__ __forceinline__ void finish_forces(typename C::R fx, typename C::R fy
 // source loads, independent across items) into shared memory; then one thread per cell sums the
 // momentum exchange in the reference's direction order and collides.
 template <class C, bool SMAG>
-__device__ __forceinline__ void body_role(const StepArgs3<C>& a, int bb) {
+__device__ __forceinline__ void body_role(const StepArgs3<C>& a, int bb, int tid) {
   using R = typename C::R;
   __shared__ R sv[Q3][32];  // pulled populations in storage units
   __shared__ R sm[Q3][32];  // momentum-exchange term of each link (0 when the link exchanges none)
-  for (int item = threadIdx.x; item < 32 * Q3; item += kStepThreads) {
+  for (int item = tid; item < 32 * Q3; item += kStepThreads) {
     const int lane = item & 31, dir = item >> 5;
     const int t = bb * 32 + lane;
     if (t >= a.nBody) continue;
@@ -431,7 +455,7 @@ __device__ __forceinline__ void body_role(const StepArgs3<C>& a, int bb) {
   }
   __syncthreads();
   R fx = R(0), fy = R(0), fz = R(0);
-  const int lane = threadIdx.x;
+  const int lane = tid;
   const int t = bb * 32 + lane;
   if (lane < 32 && t < a.nBody) do {
       const int idx = a.bodyCells[t];
@@ -439,9 +463,9 @@ __device__ __forceinline__ void body_role(const StepArgs3<C>& a, int bb) {
       const int x = meta & ((1 << 29) - 1);
       if (meta & (1 << 30)) {
         // inlet cell of a body row: equilibrium at the inflow speed
-        const R u = (R)a.st->uIn[a.par];
+        const double* eq = a.st->inletEq[a.par];
 #pragma unroll
-        for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(feq3s<C>(i, R(1), u, R(0), R(0)));
+        for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw((R)eq[i]);
         break;
       }
       const unsigned long long kinds = __ldg(a.links.kinds + t);
@@ -461,7 +485,7 @@ __device__ __forceinline__ void body_role(const StepArgs3<C>& a, int bb) {
     } while (0);
   // the momentum exchange was summed in storage units
   constexpr R IS = R(1) / R(C::SCALE);
-  if (a.sample) finish_forces<C>(fx * IS, fy * IS, fz * IS, bb, a.bodyBlocks, a.partials, a.history, a.st);
+  if (a.sample) finish_forces<C>(fx * IS, fy * IS, fz * IS, bb, a.bodyBlocks, a.partials, a.history, a.st, tid);
 }
 
 // Interior rows, one cell per thread. Interior cells pull their 19 populations from the
@@ -471,14 +495,10 @@ __device__ __forceinline__ void body_role(const StepArgs3<C>& a, int bb) {
 // loads nothing and stores the inflow equilibrium; inlet and outlet stores are short tails, paid
 // once per row.
 template <class C, bool SMAG>
-__device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int k) {
+__device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int tz) {
   using R = typename C::R;
-  const int tx = k % a.tilesX;
-  const int ty = (k / a.tilesX) % a.tilesY;
-  const int tz = k / (a.tilesX * a.tilesY);
-  const int lx = threadIdx.x % a.tileTX, ly = threadIdx.x / a.tileTX;
-  const int x = tx * a.tileTX + lx;
-  const int y = 1 + ty * a.tileTY + ly;
+  const int x = blockIdx.x * a.tileTX + threadIdx.x;
+  const int y = 1 + blockIdx.y * a.tileTY + threadIdx.y;
   const int z = 1 + tz;
   const int W = a.W, H = a.H;
   if (x >= W || y >= H - 1) return;
@@ -487,9 +507,9 @@ __device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int k) {
   if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
   if (x == 0) {
     // inlet: equilibrium at the inflow speed, no collision (step3d.ts:190-193)
-    const R u = (R)a.st->uIn[a.par];
+    const double* eq = a.st->inletEq[a.par];
 #pragma unroll
-    for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(feq3s<C>(i, R(1), u, R(0), R(0)));
+    for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw((R)eq[i]);
     return;
   }
   const bool outlet = x == W - 1;
@@ -511,16 +531,11 @@ __device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int k) {
 // rounded as a pair and stored with one 32-bit store. Cells of the pair that belong to the body role
 // are left alone.
 template <class C, bool SMAG>
-__device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int k) {
+__device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
   using R = typename C::R;
   using S = typename C::S;
-  const int tx = k % a.tilesX;
-  const int ty = (k / a.tilesX) % a.tilesY;
-  const int tz = k / (a.tilesX * a.tilesY);
-  const int tpr = a.tileTX / 2;  // threads per tile row
-  const int lx = threadIdx.x % tpr, ly = threadIdx.x / tpr;
-  const int x0 = tx * a.tileTX + 2 * lx;
-  const int y = 1 + ty * a.tileTY + ly;
+  const int x0 = blockIdx.x * a.tileTX + 2 * threadIdx.x;
+  const int y = 1 + blockIdx.y * a.tileTY + threadIdx.y;
   const int z = 1 + tz;
   const int W = a.W, H = a.H;
   if (x0 >= W || y >= H - 1) return;
@@ -554,9 +569,9 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int k) {
   if (act0) {
     if (inlet0) {
       // inlet: equilibrium at the inflow speed, no collision (step3d.ts:190-193)
-      const R u = (R)a.st->uIn[a.par];
+      const double* eq = a.st->inletEq[a.par];
 #pragma unroll
-      for (int i = 0; i < Q3; i++) o0[i] = feq3s<C>(i, R(1), u, R(0), R(0));
+      for (int i = 0; i < Q3; i++) o0[i] = (R)eq[i];
     } else {
       R f[Q3];
 #pragma unroll
@@ -591,27 +606,32 @@ constexpr int step_min_blocks(bool pair) {
 template <class C, bool SMAG, bool PAIR>
 __global__ void __launch_bounds__(kStepThreads, step_min_blocks<C>(PAIR))
     step3d_kernel(const __grid_constant__ StepArgs3<C> a) {
-  int b = blockIdx.x;
-  if (b == 0 && threadIdx.x == 0) {
-    const unsigned s = a.st->step[a.par];
-    a.st->step[a.par ^ 1] = s + 1u;
-    if (a.rampKind != 0)
-      a.st->uIn[a.par ^ 1] = ramp_speed(a.rampKind, a.rampTarget, a.rampSteps, a.rampEvery, s + 1u);
-  }
-  if (b < a.shellBlocks) {
-    shell_role<C, SMAG>(a, b);
+  // grid (tilesX, tilesY, roleZ + D - 2): the first roleZ slices of blocks hold the face and body
+  // roles (dispatched first), the others the interior tiles, one z plane per slice
+  if ((int)blockIdx.z < a.roleZ) {
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int r = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (r == 0 && tid < Q3) {
+      // the next step's counter, inlet speed and inlet equilibrium (slot par ^ 1; this step reads par)
+      const unsigned s = a.st->step[a.par];
+      if (tid == 0) a.st->step[a.par ^ 1] = s + 1u;
+      if (a.rampKind != 0) {
+        using R = typename C::R;
+        const double u = ramp_speed(a.rampKind, a.rampTarget, a.rampSteps, a.rampEvery, s + 1u);
+        if (tid == 0) a.st->uIn[a.par ^ 1] = u;
+        a.st->inletEq[a.par ^ 1][tid] = (double)feq3s<C>(tid, R(1), (R)u, R(0), R(0));
+      }
+    }
+    if (r < a.shellBlocks)
+      shell_role<C, SMAG>(a, r, tid);
+    else if (r < a.shellBlocks + a.bodyBlocks)
+      body_role<C, SMAG>(a, r - a.shellBlocks, tid);
     return;
   }
-  b -= a.shellBlocks;
-  if (b < a.bodyBlocks) {
-    body_role<C, SMAG>(a, b);
-    return;
-  }
-  b -= a.bodyBlocks;
   if constexpr (PAIR)
-    bulk_pair_role<C, SMAG>(a, b);
+    bulk_pair_role<C, SMAG>(a, blockIdx.z - a.roleZ);
   else
-    bulk_role<C, SMAG>(a, b);
+    bulk_role<C, SMAG>(a, blockIdx.z - a.roleZ);
 }
 
 // ---------------- host-side launcher ----------------
@@ -658,25 +678,29 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   // sample of zero force is still written to the ring, as the reference's reduce pass does)
   a.bodyBlocks = (L.nBody > 0 || L.sample) ? body_blocks3(L.nBody) : 0;
   const bool pair = sizeof(S) == 2 && (L.W % 2) == 0 && L.tileTX >= 64 && L.pairTiles;
+  if (!pair && L.tileTX > kStepThreads) return cudaErrorInvalidValue;
   a.tileTX = L.tileTX;
   a.tileTY = L.tileTY;
-  a.tilesX = (L.W + L.tileTX - 1) / L.tileTX;
-  a.tilesY = L.H > 2 ? (L.H - 2 + L.tileTY - 1) / L.tileTY : 0;
-  const long long tiles = (L.H > 2 && L.D > 2) ? (long long)a.tilesX * a.tilesY * (L.D - 2) : 0;
-  const long long blocks = (long long)a.shellBlocks + a.bodyBlocks + tiles;
+  const int tilesX = (L.W + L.tileTX - 1) / L.tileTX;
+  const int tilesY = L.H > 2 ? (L.H - 2 + L.tileTY - 1) / L.tileTY : 1;
+  const int zInterior = (L.H > 2 && L.D > 2) ? L.D - 2 : 0;
+  const int perSlice = tilesX * tilesY;
+  a.roleZ = (a.shellBlocks + a.bodyBlocks + perSlice - 1) / perSlice;
+  const dim3 grid(tilesX, tilesY, a.roleZ + zInterior);
+  const dim3 block(pair ? L.tileTX / 2 : L.tileTX, kStepThreads / (pair ? L.tileTX / 2 : L.tileTX), 1);
   const bool smag = L.smagC2 > 0;
   if (pair) {
     if constexpr (sizeof(S) == 2) {
       if (smag)
-        step3d_kernel<C, true, true><<<(unsigned)blocks, kStepThreads, 0, s>>>(a);
+        step3d_kernel<C, true, true><<<grid, block, 0, s>>>(a);
       else
-        step3d_kernel<C, false, true><<<(unsigned)blocks, kStepThreads, 0, s>>>(a);
+        step3d_kernel<C, false, true><<<grid, block, 0, s>>>(a);
     }
   } else {
     if (smag)
-      step3d_kernel<C, true, false><<<(unsigned)blocks, kStepThreads, 0, s>>>(a);
+      step3d_kernel<C, true, false><<<grid, block, 0, s>>>(a);
     else
-      step3d_kernel<C, false, false><<<(unsigned)blocks, kStepThreads, 0, s>>>(a);
+      step3d_kernel<C, false, false><<<grid, block, 0, s>>>(a);
   }
   return cudaGetLastError();
 }

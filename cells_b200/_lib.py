@@ -53,6 +53,27 @@ class Cells3DInfo(C.Structure):
     ]
 
 
+class Cells2DConfig(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32), ("height", C.c_int32), ("left", C.c_int32), ("right", C.c_int32),
+        ("bottom", C.c_int32), ("top", C.c_int32), ("precision", C.c_int32), ("parabolic", C.c_int32),
+        ("tau", C.c_double), ("lambda_", C.c_double), ("smagorinsky", C.c_double), ("u_in", C.c_double),
+        ("u_lid", C.c_double), ("sponge_fraction", C.c_double), ("sponge_tau", C.c_double),
+        ("body_force", C.c_double * 2), ("absorb", C.c_double), ("inlet_layer_fraction", C.c_double),
+        ("workgroup_size", C.c_int32), ("force_every", C.c_int32), ("device", C.c_int32),
+        ("fake_fail_alloc", C.c_int32), ("max_buffer_bytes", C.c_uint64), ("arithmetic", C.c_int32),
+        ("reserved1", C.c_int32),
+    ]
+
+
+class Cells2DInfo(C.Structure):
+    _fields_ = [
+        ("W", C.c_int32), ("H", C.c_int32), ("precision", C.c_int32), ("force_every", C.c_int32),
+        ("N", C.c_int64), ("step", C.c_int64), ("tile_x", C.c_int32), ("tile_y", C.c_int32),
+        ("persistent", C.c_int32), ("tunnels", C.c_int32),
+    ]
+
+
 class CellsError(RuntimeError):
     """A failed libcells call: ``status`` is the cells_status code, the message is the library's."""
 
@@ -106,6 +127,51 @@ def lib() -> C.CDLL:
         "cells3d_fake_set_force": (I, [P, D, D, D]),
         "cells_fake_live_buffers": (I64, []),
         "cells3d_mass_noalloc": (I, [P, P, I64, C.c_int32, P, P]),
+        # D2Q9 (Solver, src/solver.ts) and batches of 2D tunnels
+        "cells2d_config_default": (None, [C.POINTER(Cells2DConfig)]),
+        "cells2d_create": (I, [C.POINTER(Cells2DConfig), C.POINTER(P)]),
+        "cells2d_destroy": (None, [P]),
+        "cells2d_update": (I, [P, C.POINTER(Cells2DConfig)]),
+        "cells2d_get_config": (I, [P, C.POINTER(Cells2DConfig)]),
+        "cells2d_set_inlet": (I, [P, D]),
+        "cells2d_set_inlet_ramp": (I, [P, I, D, I64, I64]),
+        "cells2d_set_sdf": (I, [P, P, SZ]),
+        "cells2d_brush": (I, [P, D, D, D, I, I]),
+        "cells2d_brush_stroke": (I, [P, P, SZ, D, I]),
+        "cells2d_read_sdf": (I, [P, P, SZ]),
+        "cells2d_init_field": (I, [P, P]),
+        "cells2d_reset_forces": (I, [P]),
+        "cells2d_step": (I, [P, I64]),
+        "cells2d_update_macro": (I, [P]),
+        "cells2d_run": (I, [P, I64, I64]),
+        "cells2d_synchronize": (I, [P]),
+        "cells2d_read_macro": (I, [P, P]),
+        "cells2d_read_forces": (I, [P, C.POINTER(CellsForceSample), SZ, C.POINTER(SZ)]),
+        "cells2d_read_forces_begin": (I, [P]),
+        "cells2d_read_forces_end": (I, [P, C.POINTER(CellsForceSample), SZ, C.POINTER(SZ)]),
+        "cells2d_read_status": (I, [P, C.POINTER(C.c_uint32)]),
+        "cells2d_get_info": (I, [P, C.POINTER(Cells2DInfo)]),
+        "cells2d_read_params": (I, [P, P]),
+        "cells2d_mass": (I, [P, C.POINTER(D)]),
+        "cells2d_read_populations": (I, [P, P, SZ]),
+        "cells2d_write_populations": (I, [P, P, SZ]),
+        "cells2d_read_flags": (I, [P, P, SZ]),
+        "cells2d_timer_start": (I, [P]),
+        "cells2d_timer_stop": (I, [P, C.POINTER(C.c_float)]),
+        "cells2d_launch_count": (I, [P, C.POINTER(I64)]),
+        "cells2d_fake_set_force": (I, [P, D, D]),
+        "cells2d_batch_create": (I, [C.POINTER(Cells2DConfig), C.c_int32, C.POINTER(P)]),
+        "cells2d_batch_destroy": (None, [P]),
+        "cells2d_batch_tunnel": (I, [P, C.c_int32, C.POINTER(P)]),
+        "cells2d_batch_step": (I, [P, I64]),
+        "cells2d_batch_run": (I, [P, I64]),
+        "cells2d_batch_synchronize": (I, [P]),
+        "cells2d_batch_autotune": (I, [P, C.c_int32, C.POINTER(Cells2DInfo)]),
+        "cells2d_batch_set_launch": (I, [P, C.c_int32, C.c_int32, C.c_int32]),
+        "cells2d_batch_get_info": (I, [P, C.POINTER(Cells2DInfo)]),
+        "cells2d_batch_timer_start": (I, [P]),
+        "cells2d_batch_timer_stop": (I, [P, C.POINTER(C.c_float)]),
+        "cells2d_batch_launch_count": (I, [P, C.POINTER(I64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -124,6 +190,12 @@ def check(status: int, handle=None) -> None:
 def default_config3() -> Cells3DConfig:
     c = Cells3DConfig()
     lib().cells3d_config_default(C.byref(c))
+    return c
+
+
+def default_config2() -> Cells2DConfig:
+    c = Cells2DConfig()
+    lib().cells2d_config_default(C.byref(c))
     return c
 
 

@@ -32,6 +32,37 @@ def mean(v) -> float:
     return sum(v) / len(v)
 
 
+def stream_function(ux, uy, W: int, H: int) -> np.ndarray:
+    """psi[y * W + x]: u_x integrated (trapezoid) up the column x = 0, then -u_y along each row
+    (src/analysis.ts:28-37). Solid cells should carry zero velocity."""
+    ux = np.asarray(ux, dtype=np.float64).reshape(H, W)
+    uy = np.asarray(uy, dtype=np.float64).reshape(H, W)
+    psi = np.zeros((H, W))
+    psi[1:, 0] = np.cumsum(0.5 * (ux[1:, 0] + ux[:-1, 0]))
+    psi[:, 1:] = psi[:, :1] - np.cumsum(0.5 * (uy[:, 1:] + uy[:, :-1]), axis=1)
+    return psi.reshape(-1)
+
+
+def primary_vortex(psi, W: int, H: int):
+    """Interior extremum of |psi|, refined by a parabola through its neighbours on each axis
+    (src/analysis.ts:40-58). Returns (x, y, psi)."""
+    p = np.asarray(psi, dtype=np.float64).reshape(H, W)
+    inner = np.abs(p[1:H - 1, 1:W - 1])
+    by, bx = np.unravel_index(int(np.argmax(inner)), inner.shape)
+    by += 1
+    bx += 1
+    if abs(p[by, bx]) <= abs(p.reshape(-1)[1]):
+        by, bx = divmod(1, W)  # no interior value beats the reference's starting index
+
+    def refine(m, c, q):
+        den = m - 2 * c + q
+        return 0.0 if den == 0 else 0.5 * (m - q) / den
+
+    x = bx + (refine(p[by, bx - 1], p[by, bx], p[by, bx + 1]) if 0 < bx < W - 1 else 0.0)
+    y = by + (refine(p[by - 1, bx], p[by, bx], p[by + 1, bx]) if 0 < by < H - 1 else 0.0)
+    return x, y, float(p[by, bx])
+
+
 def coefficient_scale(u_target: float, area: float) -> float:
     """2 / (u^2 A), 0 without a body (src/tunnel3d.ts:75-77)."""
     return 2 / (u_target * u_target * area) if area > 0 else 0.0

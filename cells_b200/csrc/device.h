@@ -53,4 +53,12 @@ struct Device {
 // frees everything).
 extern int64_t g_fake_live_buffers;
 
+// First base of every handle type: cells_last_error reads the message through it.
+struct HandleBase {
+  std::string lastError;
+};
+
+// Message of the last failed create on this thread (cells_last_error(NULL)).
+extern thread_local std::string g_create_error;
+
 }  // namespace cells

@@ -21,7 +21,7 @@ thread_local std::string g_create_error;
 
 using namespace cells;
 
-struct Cells3D {
+struct Cells3D : HandleBase {
   Device dev;
   Cells3DConfig cfg{};
   int W = 0, H = 0, D = 0;
@@ -68,7 +68,6 @@ struct Cells3D {
   uint64_t readFirst = 0, readWritten = 0;
 
   double fakeForce[3] = {0, 0, 0};
-  std::string lastError;
 
   double lambda_value() const {
     if (std::isnan(cfg.lambda)) return std::fmin(3.0 / 16.0, 50.0 * (cfg.tau - 0.5) * (cfg.tau - 0.5));
@@ -400,7 +399,8 @@ void cells3d_config_default(Cells3DConfig* c) {
 
 const char* cells_last_error(const void* h) {
   if (!h) return g_create_error.c_str();
-  return ((const Cells3D*)h)->lastError.c_str();
+  // every handle type (Cells3D, Cells2D, Cells2DBatch) has HandleBase as its first base
+  return ((const HandleBase*)h)->lastError.c_str();
 }
 
 int cells3d_create(const Cells3DConfig* cfg, Cells3D** out) {

@@ -201,6 +201,140 @@ int cells3d_fake_set_force(Cells3D* h, double fx, double fy, double fz);
 /* Live fake-device buffers in this process (a failed create must leave this unchanged). */
 int64_t cells_fake_live_buffers(void);
 
+/* =====================================================================================
+ * D2Q9: class Solver, src/solver.ts:50-340, and batches of independent 2D tunnels.
+ *
+ * A Cells2D handle is one tunnel. cells2d_create makes a batch of one and returns its tunnel;
+ * cells2d_batch_create makes many tunnels of different sizes that advance together, one kernel
+ * launch per step for all of them (or one persistent launch for many steps), and
+ * cells2d_batch_tunnel gives a handle to each for the per-tunnel calls (geometry, parameters,
+ * readback). Stepping a tunnel of a batch of more than one is an error: step the batch.
+ * Distributions are f[i*N + x + W*y], shifted by w_i (src/shaders/step.ts:7).
+ * ===================================================================================== */
+
+/* XMode and YMode, src/lattice.ts:17-28 */
+typedef enum { CELLS_X_PERIODIC = 0, CELLS_X_WALL = 1, CELLS_X_OPEN = 2 } cells_x_mode;
+typedef enum { CELLS_Y_PERIODIC = 0, CELLS_Y_NOSLIP = 1, CELLS_Y_SLIP = 2, CELLS_Y_MOVING = 3 } cells_y_mode;
+
+/* SolverConfig, src/solver.ts:15-40. cells2d_config_default() fills the reference defaults
+ * (src/solver.ts:98-112); then set the fields you need. */
+typedef struct {
+  int32_t width, height;
+  int32_t left, right;        /* cells_x_mode; OPEN makes x = 0 a Zou-He velocity inlet and x = W-1 a
+                                 Zou-He pressure outlet (rho = 1) */
+  int32_t bottom, top;        /* cells_y_mode */
+  int32_t precision;          /* CELLS_FP32 (the reference) or CELLS_FP64 */
+  int32_t parabolic;          /* parabolic inlet profile with peak u_in (src/shaders/common.ts:39-45) */
+  double tau;
+  double lambda;              /* TRT magic parameter; default 3/16 (MAGIC_LAMBDA, src/lattice.ts:35) */
+  double smagorinsky;         /* C_s; 0 disables the subgrid model */
+  double u_in;                /* inflow speed (peak of the parabola when parabolic) */
+  double u_lid;               /* moving-wall speed */
+  double sponge_fraction;     /* fraction of the length, ending at the outlet, where tau rises */
+  double sponge_tau;
+  double body_force[2];       /* Guo body force (fx, fy) */
+  double absorb;              /* peak rate of the absorbing layers */
+  double inlet_layer_fraction;/* fraction of the length, from the inlet, with an absorbing layer */
+  int32_t workgroup_size;     /* threads per block: 64, 128 or 256; 0 = default (128) */
+  int32_t force_every;        /* sample the obstacle force every n steps; 0 disables */
+  int32_t device;             /* CUDA device ordinal, or CELLS_FAKE_DEVICE */
+  int32_t fake_fail_alloc;    /* fake device only: the n-th allocation fails (0 = none) */
+  uint64_t max_buffer_bytes;  /* largest single buffer allowed; 0 = the device's free memory */
+  int32_t arithmetic;         /* CELLS_ARITH_FAST (default) or CELLS_ARITH_EXACT */
+  int32_t reserved1;
+} Cells2DConfig;
+
+typedef struct {
+  int32_t W, H, precision, force_every;
+  int64_t N;
+  int64_t step;
+  int32_t tile_x, tile_y;     /* block shape of the batch's step kernel */
+  int32_t persistent;         /* 1 when the batch steps with the persistent kernel */
+  int32_t tunnels;            /* tunnels in the batch */
+} Cells2DInfo;
+
+typedef struct Cells2D Cells2D;
+typedef struct Cells2DBatch Cells2DBatch;
+
+void cells2d_config_default(Cells2DConfig* cfg);
+/* Solver.create (src/solver.ts:87-134): allocates, fills the SDF with 1e6 and builds the flags. On
+ * failure *out is NULL, everything allocated is freed, and allocation failures carry the message
+ * prefix "Solver allocation failed: ". */
+int cells2d_create(const Cells2DConfig* cfg, Cells2D** out);
+/* destroy (src/solver.ts:337-339). For a tunnel of a batch this releases only the handle. */
+void cells2d_destroy(Cells2D* h);
+/* update(partial) (src/solver.ts:175-178): takes a whole config, of which every field but width,
+ * height, precision, device and arithmetic may differ from the current one. */
+int cells2d_update(Cells2D* h, const Cells2DConfig* cfg);
+int cells2d_get_config(Cells2D* h, Cells2DConfig* cfg);
+int cells2d_set_inlet(Cells2D* h, double u);  /* update({ uIn: u }) */
+/* Device-side inlet ramp, as cells3d_set_inlet_ramp; update_every = 400 with SMOOTHSTEP reproduces
+ * the reference's runRamped (src/cases.ts:41-59). */
+int cells2d_set_inlet_ramp(Cells2D* h, int kind, double target, int64_t ramp_steps, int64_t update_every);
+/* setSdf (src/solver.ts:200-203): W*H floats, negative inside; rebuilds flags and refills
+ * uncovered cells. */
+int cells2d_set_sdf(Cells2D* h, const float* sdf, size_t n);
+/* brush / brushStroke (src/solver.ts:244-268): union (erase 0) or subtract (erase 1) a disc of
+ * radius r into the SDF; brush_stroke stamps n_points discs at xy[2k], xy[2k+1] and rebuilds once. */
+int cells2d_brush(Cells2D* h, double cx, double cy, double r, int erase, int rebuild);
+int cells2d_brush_stroke(Cells2D* h, const double* xy, size_t n_points, double r, int erase);
+int cells2d_read_sdf(Cells2D* h, float* out, size_t n);
+/* initField(macro?) (src/solver.ts:219-234): macro4n is (rho, ux, uy, unused) per cell, NULL = rest.
+ * Resets the tunnel's step and forces. */
+int cells2d_init_field(Cells2D* h, const float* macro4n);
+int cells2d_reset_forces(Cells2D* h);
+/* encodeSteps / encodeMacro / run (src/solver.ts:270-307); tunnels of a multi-tunnel batch step
+ * with cells2d_batch_step. */
+int cells2d_step(Cells2D* h, int64_t n);
+int cells2d_update_macro(Cells2D* h);
+int cells2d_run(Cells2D* h, int64_t n, int64_t chunk);
+int cells2d_synchronize(Cells2D* h);
+/* readMacro (src/solver.ts:309-311): 4N floats (rho, ux, uy, solid) as of the last macro refresh. */
+int cells2d_read_macro(Cells2D* h, float* out4n);
+/* readForces (src/solver.ts:314-335) with the same ring window and generation check as 3D; fz = 0. */
+int cells2d_read_forces(Cells2D* h, CellsForceSample* out, size_t cap, size_t* n_out);
+int cells2d_read_forces_begin(Cells2D* h);
+int cells2d_read_forces_end(Cells2D* h, CellsForceSample* out, size_t cap, size_t* n_out);
+/* bits: 1 non-finite force sample, 2 non-finite macro value, 4 a persistent-launch barrier timed out */
+int cells2d_read_status(Cells2D* h, uint32_t* status);
+int cells2d_get_info(Cells2D* h, Cells2DInfo* info);
+/* The 96-byte Params block as the reference packs it (src/shaders/common.ts:14-22,
+ * src/solver.ts:180-197). */
+int cells2d_read_params(Cells2D* h, void* out96);
+int cells2d_mass(Cells2D* h, double* out);
+int cells2d_read_populations(Cells2D* h, void* out, size_t bytes);
+int cells2d_write_populations(Cells2D* h, const void* in, size_t bytes);
+int cells2d_read_flags(Cells2D* h, uint32_t* out, size_t n);
+int cells2d_timer_start(Cells2D* h);
+int cells2d_timer_stop(Cells2D* h, float* ms);
+int cells2d_launch_count(Cells2D* h, int64_t* count);
+int cells2d_fake_set_force(Cells2D* h, double fx, double fy);
+
+/* ---------------- batches (no counterpart in the reference) ---------------- */
+/* count tunnels, each with its own config; precision, device and arithmetic must agree. */
+int cells2d_batch_create(const Cells2DConfig* cfgs, int32_t count, Cells2DBatch** out);
+void cells2d_batch_destroy(Cells2DBatch* b);
+/* A handle to tunnel k for the per-tunnel calls; valid until the batch is destroyed. */
+int cells2d_batch_tunnel(Cells2DBatch* b, int32_t k, Cells2D** out);
+/* n steps of every tunnel: one launch per step (replayed from CUDA graphs of 100 steps), or
+ * persistent launches of many steps when the autotuner chose that. */
+int cells2d_batch_step(Cells2DBatch* b, int64_t n);
+/* n steps, then every tunnel's macro refresh, then wait. */
+int cells2d_batch_run(Cells2DBatch* b, int64_t n);
+int cells2d_batch_synchronize(Cells2DBatch* b);
+/* Times trial_steps steps of each candidate launch shape (block shapes x per-step graphs or the
+ * persistent kernel) on a copy of the current state, keeps the fastest, and restores the state:
+ * populations, step counters, inlet speeds and force rings are as before the call. Writes the
+ * chosen shape to *info when info is not NULL. */
+int cells2d_batch_autotune(Cells2DBatch* b, int32_t trial_steps, Cells2DInfo* info);
+/* Fixes the launch shape by hand: tile_x * tile_y threads (64, 128 or 256, tile_x a multiple of 32),
+ * persistent 0 or 1. */
+int cells2d_batch_set_launch(Cells2DBatch* b, int32_t tile_x, int32_t tile_y, int32_t persistent);
+int cells2d_batch_get_info(Cells2DBatch* b, Cells2DInfo* info);
+int cells2d_batch_timer_start(Cells2DBatch* b);
+int cells2d_batch_timer_stop(Cells2DBatch* b, float* ms);
+int cells2d_batch_launch_count(Cells2DBatch* b, int64_t* count);
+
 #ifdef __cplusplus
 }
 #endif

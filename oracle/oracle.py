@@ -30,6 +30,14 @@ class HostParams3(C.Structure):
                 ("spongeStart", C.c_double), ("tauSponge", C.c_double), ("absorb", C.c_double)]
 
 
+class HostParams2(C.Structure):
+    _fields_ = [("W", C.c_int32), ("H", C.c_int32), ("left", C.c_int32), ("right", C.c_int32),
+                ("bottom", C.c_int32), ("top", C.c_int32), ("parabolic", C.c_int32), ("forcing", C.c_int32),
+                ("tau", C.c_double), ("lambda_", C.c_double), ("smagC2", C.c_double), ("uIn", C.c_double),
+                ("spongeStart", C.c_double), ("tauSponge", C.c_double), ("uLid", C.c_double), ("fx", C.c_double),
+                ("fy", C.c_double), ("absorb", C.c_double), ("inletLayer", C.c_double)]
+
+
 _lib = None
 
 
@@ -56,6 +64,17 @@ def lib():
         L.oracle_codec_roundtrip.restype = C.c_float
         L.oracle_num_threads.restype = C.c_int
         for fn in ("oracle3d_step", "oracle3d_flags", "oracle3d_init", "oracle3d_macro", "oracle3d_mass"):
+            getattr(L, fn).restype = C.c_int
+        HP2 = C.POINTER(HostParams2)
+        L.oracle2d_step.argtypes = [C.c_int, HP2, P, P, P, P, P]
+        L.oracle2d_run.argtypes = [C.c_int, HP2, P, P, C.c_int, C.c_longlong, P, P]
+        L.oracle2d_flags.argtypes = [C.c_int, HP2, P, P, P, P, P]
+        L.oracle2d_init.argtypes = [C.c_int, HP2, P, P, P]
+        L.oracle2d_macro.argtypes = [C.c_int, HP2, P, P, P]
+        L.oracle2d_mass.argtypes = [C.c_int, HP2, P, P, C.POINTER(C.c_double)]
+        L.oracle2d_brush.argtypes = [C.c_int, C.c_int, P, C.c_double, C.c_double, C.c_double, C.c_int]
+        for fn in ("oracle2d_step", "oracle2d_run", "oracle2d_flags", "oracle2d_init", "oracle2d_macro",
+                   "oracle2d_mass", "oracle2d_brush"):
             getattr(L, fn).restype = C.c_int
         _lib = L
     return _lib
@@ -168,6 +187,130 @@ class OracleSolver3D:
         p = self.params()
         v = C.c_double()
         lib().oracle3d_mass(self.prec, C.byref(p), _ptr(self.f[self.parity]), _ptr(self.flags), C.byref(v))
+        return v.value
+
+
+class OracleSolver2D:
+    """The reference Solver's host logic (src/solver.ts:50-340) over the CPU restatement of its
+    kernels (oracle/lbm2d.cpp). Config keys follow SolverConfig (src/solver.ts:15-40)."""
+
+    HISTORY_LEN = 8192
+    DEFAULTS = dict(lambda_=3 / 16, smagorinsky=0.0, uIn=0.0, parabolic=False, uLid=0.0, spongeFraction=0.0,
+                    spongeTau=1.0, bodyForce=(0.0, 0.0), absorb=0.0, inletLayerFraction=0.0, forceEvery=1)
+
+    def __init__(self, width, height, left=0, right=0, bottom=0, top=0, tau=0.6, precision="fp32", **cfg):
+        self.W, self.H = width, height
+        self.N = width * height
+        self.precision = precision
+        self.prec = PREC[precision]
+        if self.prec not in (0, 3):
+            raise ValueError("the 2D oracle stores fp32 or fp64")
+        self.cfg = dict(self.DEFAULTS)
+        self.cfg.update(left=left, right=right, bottom=bottom, top=top, tau=tau)
+        self.cfg.update(cfg)
+        dt = DTYPE[precision]
+        self.f = [np.zeros(9 * self.N, dtype=dt), np.zeros(9 * self.N, dtype=dt)]
+        self.flags = np.zeros(self.N, dtype=np.uint32)
+        self.sdf = np.full(self.N, 1e6, dtype=np.float32)
+        self.macro = np.zeros(4 * self.N, dtype=np.float32)
+        self.cell_force = np.zeros(2 * self.N, dtype=np.float64)
+        self.step = 0
+        self.parity = 0
+        self.samples = []
+        self._rebuild_flags()
+
+    # writeParams, src/solver.ts:180-197
+    def params(self) -> HostParams2:
+        c = self.cfg
+        p = HostParams2()
+        p.W, p.H = self.W, self.H
+        p.left, p.right, p.bottom, p.top = c["left"], c["right"], c["bottom"], c["top"]
+        p.tau = c["tau"]
+        p.lambda_ = c["lambda_"]
+        p.smagC2 = c["smagorinsky"] * c["smagorinsky"]
+        p.uIn = c["uIn"]
+        p.parabolic = 1 if c["parabolic"] else 0
+        p.spongeStart = (self.W - 1) * (1 - c["spongeFraction"]) if c["spongeFraction"] > 0 else 1e9
+        p.tauSponge = max(c["spongeTau"], c["tau"])
+        p.uLid = c["uLid"]
+        p.fx, p.fy = c["bodyForce"]
+        p.forcing = 1 if (c["bodyForce"][0] != 0 or c["bodyForce"][1] != 0) else 0
+        p.absorb = c["absorb"]
+        p.inletLayer = c["inletLayerFraction"] * (self.W - 1)
+        return p
+
+    def update(self, **changes):
+        self.cfg.update(changes)
+
+    def _macro(self):
+        p = self.params()
+        lib().oracle2d_macro(self.prec, C.byref(p), _ptr(self.f[self.parity]), _ptr(self.flags), _ptr(self.macro))
+
+    def _rebuild_flags(self):
+        self._macro()
+        p = self.params()
+        lib().oracle2d_flags(self.prec, C.byref(p), _ptr(self.sdf), _ptr(self.flags), _ptr(self.f[0]),
+                             _ptr(self.f[1]), _ptr(self.macro))
+
+    def setSdf(self, sdf):
+        self.sdf = np.ascontiguousarray(sdf, dtype=np.float32).copy()
+        self._rebuild_flags()
+
+    def brush(self, cx, cy, r, erase, rebuild=True):
+        lib().oracle2d_brush(self.W, self.H, _ptr(self.sdf), cx, cy, r, 1 if erase else 0)
+        if rebuild:
+            self._rebuild_flags()
+
+    def initField(self, macro=None):
+        if macro is None:
+            macro = np.zeros(4 * self.N, dtype=np.float32)
+            macro[0::4] = 1.0
+        m = np.ascontiguousarray(macro, dtype=np.float32)
+        self.macro = m.copy()
+        p = self.params()
+        lib().oracle2d_init(self.prec, C.byref(p), _ptr(m), _ptr(self.f[0]), _ptr(self.f[1]))
+        self.step = 0
+        self.parity = 0
+        self.samples = []
+
+    def encodeSteps(self, n):
+        every = self.cfg["forceEvery"]
+        if every <= 0:
+            p = self.params()
+            self.parity = lib().oracle2d_run(self.prec, C.byref(p), _ptr(self.f[0]), _ptr(self.f[1]), self.parity, n,
+                                             _ptr(self.flags), _ptr(self.sdf))
+            self.step += n
+            return
+        for _ in range(n):
+            p = self.params()
+            sample = (self.step + 1) % every == 0
+            lib().oracle2d_step(self.prec, C.byref(p), _ptr(self.f[self.parity]), _ptr(self.f[self.parity ^ 1]),
+                                _ptr(self.flags), _ptr(self.sdf), _ptr(self.cell_force) if sample else None)
+            self.parity ^= 1
+            self.step += 1
+            if sample:
+                fsum = self.cell_force.reshape(-1, 2).sum(axis=0)
+                self.samples.append((self.step, float(fsum[0]), float(fsum[1])))
+
+    def run(self, n, chunk=500):
+        self.encodeSteps(n)
+        self._macro()
+
+    def readMacro(self):
+        return self.macro.copy()
+
+    def readForces(self):
+        out = self.samples[-self.HISTORY_LEN:]
+        self.samples = []
+        return [{"step": s, "fx": a, "fy": b} for s, a, b in out]
+
+    def populations(self):
+        return self.f[self.parity]
+
+    def mass(self):
+        p = self.params()
+        v = C.c_double()
+        lib().oracle2d_mass(self.prec, C.byref(p), _ptr(self.f[self.parity]), _ptr(self.flags), C.byref(v))
         return v.value
 
 

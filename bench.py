@@ -179,6 +179,55 @@ def run_e2e(s, sdf, macro, steps: int, chunk: int = 100):
     return dt, h2d, d2h
 
 
+def precision_cd(device, steps=5000, grid=(192, 96, 96)):
+    """C_D of the sphere tunnel (mean over the last 1000 of `steps` steps) per storage precision,
+    and its relative error against the FP64 run of the same kernel and grid."""
+    import numpy as np
+
+    W, H, D = grid
+    d = 16 * H / 96
+    scale = 2 / (0.1 * 0.1 * np.pi * d * d / 4)
+    out = {}
+    for prec in ("fp64", "fp32", "fp16", "bf16"):
+        s, sdf, macro, _ = tunnel_setup(W, H, D, prec, device=device)
+        s.setSdf(sdf)
+        s.initField(macro)
+        s.setInletRamp("linear", 0.1, 3000, 1)
+        s.encodeSteps(steps)
+        f = s.readForcesArray()
+        s.destroy()
+        out[prec] = scale * float(np.mean(f[f[:, 0] > steps - 1000, 1]))
+    ref = out["fp64"]
+    return {"workload": f"D3Q19 {W}x{H}x{D} sphere d={d:g} Re200, {steps} steps, C_D over the last 1000",
+            "C_D": {k: round(v, 6) for k, v in out.items()},
+            "rel_err_vs_fp64": {k: abs(v - ref) / abs(ref) for k, v in out.items() if k != "fp64"}}
+
+
+def adjoint_cost(device):
+    """Wall time of the adjoint's backward sweep (recompute + adjoint steps) over one plain forward
+    run of the same 6000 steps, on the 128x64x64 star-body drag problem (FP32)."""
+    from cells_b200.adjoint import StarDrag
+    from cells_b200.rng import SEED, normal
+
+    p = StarDrag(precision="fp32", device=device)
+    J = p.forward(0.02 * normal(SEED, 17, 16))
+    p.solver.synchronize()
+    t0 = time.perf_counter()
+    dcoef, du = p.backward()
+    t_bwd = time.perf_counter() - t0
+    s = p.solver
+    s.initField(p.macro)
+    s.setInletRamp("linear", 0.1, p.ramp_steps, 1)
+    s.synchronize()
+    t0 = time.perf_counter()
+    s.encodeSteps(p.steps)
+    s.synchronize()
+    t_fwd = time.perf_counter() - t0
+    p.destroy()
+    return {"workload": "star body r0=12 at 128x64x64, Re150, 6000 steps, K=100, FP32", "J": J,
+            "forward_s": t_fwd, "backward_s": t_bwd, "cost_ratio": t_bwd / t_fwd, "dJ_du": du}
+
+
 def cpu_baseline(W, H, D, precision="fp32", budget_s=12.0, max_steps=400):
     """The oracle (C++ restatement of the reference's kernels) on the host cores, OpenMP."""
     from cells_b200 import geometry as g
@@ -251,8 +300,6 @@ def main():
             dist.destroy_process_group()
         return
 
-    from cells_b200 import analysis
-
     s, sdf, macro, tau = tunnel_setup(W, H, D, args.precision, device=local)
     s.setSdf(sdf)
     s.initField(macro)
@@ -293,7 +340,6 @@ def main():
         line["e2e"] = {"value": round(N * e2e_steps / dt / 1e6 * world, 1), "unit": "MLUPS",
                        "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
                        "steps": e2e_steps, "calls": "setSdf, initField, (setInlet, run(100), readForces) x k, readMacro"}
-        f = s.readForcesArray()
         s.destroy()
         variants = []
         for prec, grid in (("fp16", (W, H, D)), ("bf16", (W, H, D)), ("fp64", (W, H, D)),
@@ -309,6 +355,16 @@ def main():
                              "hbm_frac": round(vm * 1e6 * BYTES_PER_CELL[prec] / 1e9 / hbm, 4)})
             v.destroy()
         line["variants"] = variants
+        from cells_b200 import cases2d
+
+        line["precision_cd"] = precision_cd(local)
+        b2 = cases2d.batched_naca_throughput(10000, device=local)
+        b2["hbm_frac"] = round(b2["batched_mlups"] * 1e6 * 72 / 1e9 / hbm, 4)
+        line["batched2d"] = b2
+        c2 = cases2d.cylinder_tunnel(20000, device=local)
+        line["cylinder2d"] = {"workload": "D2Q9 400x100 cylinder D=20 Re100, 20000 steps", "mlups": c2["mlups"],
+                              "C_D": c2["C_D"], "C_L_amp": c2["C_L_amp"], "St": c2["St"]}
+        line["adjoint"] = adjoint_cost(local)
         if rank == 0 and world == 1:
             line["cpu_baseline"] = cpu_baseline(W, H, D, args.precision)
     else:

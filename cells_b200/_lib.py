@@ -74,6 +74,11 @@ class Cells2DInfo(C.Structure):
     ]
 
 
+class Cells3DAdjointSpec(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("window_begin", C.c_int64), ("window_end", C.c_int64),
+                ("checkpoint_every", C.c_int32), ("component", C.c_int32), ("scale", C.c_double)]
+
+
 class CellsError(RuntimeError):
     """A failed libcells call: ``status`` is the cells_status code, the message is the library's."""
 
@@ -127,6 +132,9 @@ def lib() -> C.CDLL:
         "cells3d_fake_set_force": (I, [P, D, D, D]),
         "cells_fake_live_buffers": (I64, []),
         "cells3d_mass_noalloc": (I, [P, P, I64, C.c_int32, P, P]),
+        "cells3d_adjoint_forward": (I, [P, C.POINTER(Cells3DAdjointSpec), C.POINTER(D)]),
+        "cells3d_adjoint_backward": (I, [P, P, P, C.POINTER(D), P]),
+        "cells3d_adjoint_release": (I, [P]),
         # D2Q9 (Solver, src/solver.ts) and batches of 2D tunnels
         "cells2d_config_default": (None, [C.POINTER(Cells2DConfig)]),
         "cells2d_create": (I, [C.POINTER(Cells2DConfig), C.POINTER(P)]),

@@ -1,0 +1,132 @@
+"""3D validation and precision workloads on the CUDA solver.
+
+* ``sphere_fp16``: the reference's sphereFp16 case (src/cases3d.ts:11-81): a sphere of diameter 16 at
+  Re 100 on 192x96x96, FP32 and FP16 storage each run in blocks of 2000 steps (smoothstep inlet ramp
+  over 3000 steps set per chunk of 400, forces every 4 steps) until C_D changes by less than 1e-4
+  between blocks; gate: C_D of FP16 within 1% of FP32. BF16 and FP64 are added beside them.
+* ``precision_sweep``: four obstacles (sphere D=20, cube edge 18, spanwise cylinder D=16, NACA0012
+  wing chord 40 over the full span at 6 degrees) at Re 200 on 256x128x128, stored as FP32, FP16
+  and BF16 with FP32 arithmetic, 4000 steps; time-averaged C_D and C_L over steps 2000..4000 and the
+  relative velocity L2 over fluid cells at step 4000, each against an FP64 run of the same kernel on
+  the same grid and on the 128x64x64 grid with lengths halved (same Re and u).
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+from . import analysis, geometry as g
+from .rng import perturbed_rest3
+from .solver3d import Solver3D
+from .units import derive_tau
+
+
+def smoothstep(t):
+    return t * t * (3 - 2 * t)
+
+
+def sphere_fp16(precisions=("fp32", "fp16", "bf16", "fp64"), device=0, grid=(192, 96, 96), max_blocks=15):
+    W, H, D = grid
+    d, u = 16, 0.1
+    tau = derive_tau(100, u, d).tau
+    sdf = g.empty_sdf3(W, H, D)
+    g.add_sphere(sdf, W, H, D, W / 4, H / 2, D / 2, d / 2)
+    scale = 2 / (u * u * g.reference_area("sphere", d, D))
+    cd, steps = {}, {}
+    for prec in precisions:
+        s = Solver3D.create(W, H, D, precision=prec, tau=tau, spongeFraction=0.15, spongeTau=1.0, absorb=0.02,
+                            forceEvery=4, device=device)
+        s.setSdf(sdf)
+        s.initField()
+        prev = math.nan
+        for k in range(1, max_blocks + 1):
+            block = []
+            end = k * 2000
+            while s.step < end:
+                s.setInlet(u * smoothstep(min(1.0, s.step / 3000)))
+                s.run(min(400, end - s.step), 400)
+                block.extend(f["fx"] for f in s.readForces())
+            c = analysis.mean(block) * scale
+            cd[prec] = c
+            if k >= 5 and abs(c - prev) / abs(prev) < 1e-4:
+                break
+            prev = c
+        steps[prec] = s.step
+        s.destroy()
+    ref = cd["fp32"]
+    return {"name": "Sphere C_D, FP16 vs FP32 (Re 100)", "C_D": cd, "steps": steps,
+            "rel_vs_fp32": {p: abs(v - ref) / abs(ref) for p, v in cd.items()},
+            "pass": abs(cd["fp16"] - ref) / abs(ref) <= 0.01 if "fp16" in cd else None}
+
+
+OBSTACLES = (("sphere", 20, 0.0), ("cube", 18, 0.0), ("cylinder", 16, 0.0), ("wing", 40, 6.0))
+
+
+def _body(kind, size, angle_deg, W, H, D):
+    cx, cy, cz = W / 4, H / 2, D / 2
+    sdf = g.empty_sdf3(W, H, D)
+    a = math.radians(angle_deg)
+    if kind == "sphere":
+        g.add_sphere(sdf, W, H, D, cx, cy, cz, size / 2)
+        area = g.reference_area("sphere", size, D)
+    elif kind == "cube":
+        g.add_box3(sdf, W, H, D, cx, cy, cz, size / 2, size / 2, size / 2, 0.0)
+        area = g.reference_area("cube", size, D)
+    elif kind == "cylinder":
+        g.add_cylinder_z(sdf, W, H, D, cx, cy, size / 2)
+        area = g.reference_area("cylinder", size, D)
+    else:
+        g.add_wing(sdf, W, H, D, cx, cy, cz, size, D, a)
+        area = g.reference_area("wing", size, D, span=D)
+    return sdf, area
+
+
+def _run(kind, size, angle, grid, precision, steps, device, u=0.1, re=200.0):
+    W, H, D = grid
+    sdf, area = _body(kind, size, angle, W, H, D)
+    tau = max(derive_tau(re, u, size).tau, 0.51)
+    s = Solver3D.create(W, H, D, precision=precision, tau=tau, uIn=0.0, spongeFraction=0.15, spongeTau=1.0,
+                        absorb=0.02, forceEvery=1, device=device)
+    s.setSdf(sdf)
+    s.initField(perturbed_rest3(W, H, D, 1e-4))
+    s.setInletRamp("linear", u, 3000 * steps // 4000, 1)
+    s.encodeSteps(steps)
+    f = s.readForcesArray()
+    s.run(0)
+    m = s.readMacro().reshape(-1, 4)
+    s.destroy()
+    scale = 2 / (u * u * area)
+    sel = f[:, 0] > steps // 2
+    return {"C_D": scale * float(np.mean(f[sel, 1])), "C_L": scale * float(np.mean(f[sel, 2])), "macro": m,
+            "tau": tau}
+
+
+def _vel_l2(a, b):
+    fluid = (b[:, 3] != 0) & (a[:, 3] != 0)
+    du = a[fluid, :3].astype(np.float64) - b[fluid, :3].astype(np.float64)
+    return math.sqrt(float(np.sum(du * du)) / float(np.sum(b[fluid, :3].astype(np.float64) ** 2)))
+
+
+def precision_sweep(device=0, grid=(256, 128, 128), steps=4000, obstacles=OBSTACLES,
+                    precisions=("fp32", "fp16", "bf16")):
+    W, H, D = grid
+    half = (W // 2, H // 2, D // 2)
+    out = []
+    for kind, size, angle in obstacles:
+        t0 = time.perf_counter()
+        ref = _run(kind, size, angle, grid, "fp64", steps, device)
+        ref_half = _run(kind, size / 2, angle, half, "fp64", steps // 2, device)
+        row = {"obstacle": kind, "size": size, "tau": ref["tau"], "fp64": {"C_D": ref["C_D"], "C_L": ref["C_L"]},
+               "fp64_half_grid": {"C_D": ref_half["C_D"], "C_L": ref_half["C_L"]}}
+        for prec in precisions:
+            r = _run(kind, size, angle, grid, prec, steps, device)
+            row[prec] = {"C_D": r["C_D"], "C_L": r["C_L"],
+                         "C_D_err_vs_fp64": abs(r["C_D"] - ref["C_D"]) / abs(ref["C_D"]),
+                         "C_L_abs_err_vs_fp64": abs(r["C_L"] - ref["C_L"]),
+                         "C_D_err_vs_fp64_half_grid": abs(r["C_D"] - ref_half["C_D"]) / abs(ref_half["C_D"]),
+                         "vel_L2_vs_fp64": _vel_l2(r["macro"], ref["macro"])}
+        row["seconds"] = time.perf_counter() - t0
+        out.append(row)
+    return out

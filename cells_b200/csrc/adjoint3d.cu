@@ -1,0 +1,766 @@
+// Discrete adjoint of the D3Q19 step: the adjoint step kernels, the recorded forward run with
+// checkpoints, the backward sweep with recomputation, and their C ABI (include/cells.h). No
+// counterpart in the reference.
+//
+// Adjoint step n (from lambda^{n+1} to lambda^n over the recomputed state f^n), per cell x:
+//   g = P(f^n)(x): the 19 pulled values (plain pulls, or the cell's link records at boundaries);
+//   lambda_g = (dC/dg)^T lambda^{n+1}(x): the transposed Jacobian of the TRT collision (or of the
+//     outlet's feq(1, u), or zero at the inlet, whose output does not depend on g);
+//   the streaming transpose: a plain pull of direction i from x - c_i is the only regular reader of
+//     that element, so lambda^n_i(x - c_i) = lambda_g,i is a plain store; a link's adjoint goes to
+//     lamG and a second kernel adds it, with the objective's direct force terms, to the link's
+//     source elements (a fixed-order sum per element: deterministic).
+// Shape: dJ/dq per Bouzidi link accumulates (lambda_g + w cF) dg/dq; dq/dsdf then gives dJ/dsdf.
+// Inflow: dJ/du_n from the inlet's feq(1, u_n) and the absorbing layer's target u_n, summed per
+// step in f64 with a fixed order.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "adjoint3d.h"
+#include "solver3d_state.h"
+
+using namespace cells;
+
+namespace {
+
+__host__ __device__ __forceinline__ long long off3(int i, int W, int H) {
+  return (long long)cx3(i) + (long long)W * ((long long)cy3(i) + (long long)H * cz3(i));
+}
+
+template <class R>
+struct XRow {
+  R omP, omM, sigma;
+};
+
+// (dC/dg)^T lp for the TRT collision with sponge rate omP/omM and absorbing strength sigma toward
+// the inflow speed ut (src/shaders/step3d.ts:38-102, Smagorinsky off). Also returns dJ/dut.
+template <class R>
+__device__ __forceinline__ void collide_adjoint3(const R g[Q3], const R lp[Q3], R omP, R omM, R sigma, R ut,
+                                                 R lg[Q3], R& dut) {
+  R drho = R(0);
+#pragma unroll
+  for (int i = 0; i < Q3; i++) drho += g[i];
+  const R rho = R(1) + drho;
+  const R inv = R(1) / rho;
+  R jx = R(0), jy = R(0), jz = R(0);
+#pragma unroll
+  for (int i = 1; i < Q3; i++) {
+    jx += R(cx3(i)) * g[i];
+    jy += R(cy3(i)) * g[i];
+    jz += R(cz3(i)) * g[i];
+  }
+  const R ux = jx * inv, uy = jy * inv, uz = jz * inv;
+  const R uu = ux * ux + uy * uy + uz * uz;
+  const R usq = R(1.5) * uu;
+  const R w0 = w3<R>(0);
+  R rhoB = R(0), usqB = R(0), uxB = R(0), uyB = R(0), uzB = R(0), dqB = R(0), utB = R(0);
+  lg[0] = lp[0] * (R(1) - omP);
+  {
+    const R e0 = omP * lp[0];
+    rhoB += e0 * w0 * (R(1) - usq);
+    usqB -= e0 * w0 * rho;
+  }
+  const bool absorb = sigma > R(0);
+  if (absorb) dqB -= lp[0] * sigma * w0;
+#pragma unroll
+  for (int a = 1; a < Q3; a += 2) {
+    const int b = a + 1;
+    const R wa = w3<R>(a);
+    const R cu = R(3) * (R(cx3(a)) * ux + R(cy3(a)) * uy + R(cz3(a)) * uz);
+    const R S = lp[a] + lp[b];
+    const R Dd = lp[a] - lp[b];
+    lg[a] = lp[a] - R(0.5) * omP * S - R(0.5) * omM * Dd;
+    lg[b] = lp[b] - R(0.5) * omP * S + R(0.5) * omM * Dd;
+    const R eS = omP * S, eA = omM * Dd;
+    rhoB += eS * wa * (R(1) + R(0.5) * cu * cu - usq) + eA * wa * cu;
+    R cuB = eS * wa * rho * cu + eA * wa * rho;
+    usqB -= eS * wa * rho;
+    if (absorb) {
+      const R cut = R(3) * R(cx3(a)) * ut;
+      const R sw = sigma * wa;
+      rhoB += S * sw * R(0.5) * (cut * cut - cu * cu) + Dd * sw * (cut - cu);
+      cuB -= S * sw * rho * cu + Dd * sw * rho;
+      dqB -= S * sw;
+      utB += R(3) * R(cx3(a)) * (S * sw * rho * cut + Dd * sw * rho);
+    }
+    uxB += R(3) * R(cx3(a)) * cuB;
+    uyB += R(3) * R(cy3(a)) * cuB;
+    uzB += R(3) * R(cz3(a)) * cuB;
+  }
+  if (absorb) {  // dq = 1.5 rho (ut^2 - |u|^2)
+    rhoB += dqB * R(1.5) * (ut * ut - uu);
+    uxB -= dqB * R(3) * rho * ux;
+    uyB -= dqB * R(3) * rho * uy;
+    uzB -= dqB * R(3) * rho * uz;
+    utB += dqB * R(3) * rho * ut;
+  }
+  uxB += R(3) * ux * usqB;
+  uyB += R(3) * uy * usqB;
+  uzB += R(3) * uz * usqB;
+  const R jxB = uxB * inv, jyB = uyB * inv, jzB = uzB * inv;
+  rhoB -= (ux * uxB + uy * uyB + uz * uzB) * inv;
+#pragma unroll
+  for (int i = 0; i < Q3; i++) lg[i] += rhoB + R(cx3(i)) * jxB + R(cy3(i)) * jyB + R(cz3(i)) * jzB;
+  dut = utB;
+}
+
+// (d feq(1, u(g)) / dg)^T lp: the outlet stores feq(1, u) with u the velocity of the pulled values.
+template <class R>
+__device__ __forceinline__ void outlet_adjoint3(const R g[Q3], const R lp[Q3], R lg[Q3]) {
+  R drho = R(0);
+#pragma unroll
+  for (int i = 0; i < Q3; i++) drho += g[i];
+  const R rho = R(1) + drho;
+  const R inv = R(1) / rho;
+  R jx = R(0), jy = R(0), jz = R(0);
+#pragma unroll
+  for (int i = 1; i < Q3; i++) {
+    jx += R(cx3(i)) * g[i];
+    jy += R(cy3(i)) * g[i];
+    jz += R(cz3(i)) * g[i];
+  }
+  const R ux = jx * inv, uy = jy * inv, uz = jz * inv;
+  R uxB = R(0), uyB = R(0), uzB = R(0);
+#pragma unroll
+  for (int i = 0; i < Q3; i++) {
+    const R cu = R(3) * (R(cx3(i)) * ux + R(cy3(i)) * uy + R(cz3(i)) * uz);
+    const R k = lp[i] * w3<R>(i);
+    uxB += k * (R(3) * R(cx3(i)) * (R(1) + cu) - R(3) * ux);
+    uyB += k * (R(3) * R(cy3(i)) * (R(1) + cu) - R(3) * uy);
+    uzB += k * (R(3) * R(cz3(i)) * (R(1) + cu) - R(3) * uz);
+  }
+  const R jxB = uxB * inv, jyB = uyB * inv, jzB = uzB * inv;
+  const R rhoB = -(ux * uxB + uy * uyB + uz * uzB) * inv;
+#pragma unroll
+  for (int i = 0; i < Q3; i++) lg[i] = rhoB + R(cx3(i)) * jxB + R(cy3(i)) * jyB + R(cz3(i)) * jzB;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kAdjThreads) adj_cells3_kernel(AdjLaunch3 a) {
+  __shared__ double red[kAdjThreads / 32];
+  __shared__ bool last;
+  const long long N = a.N;
+  const long long idx = (long long)blockIdx.x * kAdjThreads + threadIdx.x;
+  const R* __restrict__ f = (const R*)a.f;
+  const R* __restrict__ lamNext = (const R*)a.lamNext;
+  R* __restrict__ lamOut = (R*)a.lamOut;
+  double du = 0.0;
+  if (idx < N) {
+    const uint32_t fl = a.flags[idx];
+    if (!(fl & FLAG3_SOLID)) {
+      R lp[Q3];
+#pragma unroll
+      for (int i = 0; i < Q3; i++) lp[i] = lamNext[i * N + idx];
+      const R u = (R)a.u;
+      if (fl & FLAG3_INLET) {
+        // f' = feq(1, u, 0, 0): d/du = w_i (3 c_ix + 9 c_ix^2 u - 3 u)
+        R s = R(0);
+#pragma unroll
+        for (int i = 0; i < Q3; i++) {
+          const R c = R(cx3(i));
+          s += lp[i] * w3<R>(i) * (R(3) * c + R(9) * c * c * u - R(3) * u);
+        }
+        du = (double)s;
+      } else {
+        const int W = a.W, H = a.H;
+        const int base = fl ? a.linkBase[idx] : -1;
+        const R* la1 = (const R*)a.la1;
+        const R* la2 = (const R*)a.la2;
+        R g[Q3];
+        int rank = 0;
+#pragma unroll
+        for (int i = 0; i < Q3; i++) {
+          if (i == 0 || !(fl & (1u << i))) {
+            g[i] = f[i * N + idx - off3(i, W, H)];
+          } else {
+            const int k = base + rank++;
+            const long long e2 = a.le2[k];
+            g[i] = la1[k] * f[a.le1[k]] + (e2 >= 0 ? la2[k] * f[e2] : R(0));
+          }
+        }
+        R lg[Q3];
+        if (fl & FLAG3_OUTLET) {
+          outlet_adjoint3<R>(g, lp, lg);
+        } else {
+          const int x = (int)(idx % W);
+          const R* xt = (const R*)a.xTab + 4 * x;
+          R dut = R(0);
+          collide_adjoint3<R>(g, lp, xt[0], xt[1], xt[2], u, lg, dut);
+          du = (double)dut;
+        }
+        const R* lcF = (const R*)a.lcF;
+        const R* lq = (const R*)a.lq;
+        R* lamG = (R*)a.lamG;
+        const R w = (R)a.w;
+        rank = 0;
+#pragma unroll
+        for (int i = 0; i < Q3; i++) {
+          if (i == 0 || !(fl & (1u << i))) {
+            lamOut[i * N + idx - off3(i, W, H)] = lg[i];
+          } else {
+            const int k = base + rank++;
+            lamG[k] = lg[i];
+            const int qk = a.lqk[k];
+            if (qk) {
+              const R fj = f[a.le1[k]], f2 = f[a.le2[k]], q = lq[k];
+              const R dgdq = qk == 1 ? R(2) * (fj - f2) : (f2 - fj) / (R(2) * q * q);
+              a.dqAcc[k] += (double)((lg[i] + w * lcF[k]) * dgdq);
+            }
+          }
+        }
+      }
+    }
+  }
+  // dJ/du_n: block sums in f64, then the last block sums the partials in block order
+  for (int o = 16; o > 0; o >>= 1) du += __shfl_down_sync(0xffffffffu, du, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = du;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < kAdjThreads / 32; k++) s += red[k];
+    a.blockPart[blockIdx.x] = s;
+    __threadfence();
+    last = atomicAdd(a.counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double s = 0.0;
+  for (unsigned k = threadIdx.x; k < gridDim.x; k += kAdjThreads) s += __ldcg(&a.blockPart[k]);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < kAdjThreads / 32; k++) t += red[k];
+    *a.dudOut = t;
+    *a.counter = 0u;
+  }
+}
+
+// Elements with an irregular reader or no regular reader: lambda^n[e] (= 0 when no regular reader
+// wrote it) plus each link's adjoint times its coefficient, plus the direct force terms.
+template <class R>
+__global__ void __launch_bounds__(256) adj_rows3_kernel(AdjLaunch3 a) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= a.nRows) return;
+  R* lamOut = (R*)a.lamOut;
+  const R* lamG = (const R*)a.lamG;
+  const R* lcF = (const R*)a.lcF;
+  const R* alpha = (const R*)a.entAlpha;
+  const R w = (R)a.w;
+  const long long e = a.rowElem[r];
+  R v = a.rowSet[r] ? R(0) : lamOut[e];
+  for (int k = a.rowStart[r]; k < a.rowStart[r + 1]; k++) {
+    const int L = a.entLink[k];
+    v += alpha[k] * (lamG[L] + w * lcF[L]);
+  }
+  v += w * ((const R*)a.rowPhi)[r];
+  lamOut[e] = v;
+}
+
+template <class R>
+cudaError_t launch_adjoint_step3_t(const AdjLaunch3& a, cudaStream_t s) {
+  const unsigned blocks = (unsigned)((a.N + kAdjThreads - 1) / kAdjThreads);
+  adj_cells3_kernel<R><<<blocks, kAdjThreads, 0, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || a.nRows == 0) return e;
+  adj_rows3_kernel<R><<<(unsigned)((a.nRows + 255) / 256), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+namespace cells {
+cudaError_t launch_adjoint_step3(int precision, const AdjLaunch3& a, cudaStream_t s) {
+  if (precision == 0) return launch_adjoint_step3_t<float>(a, s);
+  if (precision == 3) return launch_adjoint_step3_t<double>(a, s);
+  return cudaErrorInvalidValue;
+}
+}  // namespace cells
+
+// ---------------- host: link resolution (the rules of pullSlow3, src/shaders/step3d.ts:119-168) ----
+
+namespace {
+
+template <class R>
+void resolve_links(const Cells3D* h, const std::vector<uint32_t>& fl, const std::vector<float>& sdf, int comp,
+                   std::vector<int>& base, std::vector<AdjLink3Host>& links) {
+  const int W = h->W, H = h->H, D = h->D;
+  const long long N = h->N;
+  auto at = [&](int x, int y, int z) { return (long long)x + (long long)W * ((long long)y + (long long)H * z); };
+  auto solid = [&](long long c) { return (fl[(size_t)c] & FLAG3_SOLID) != 0u; };
+  auto cc = [&](int j) { return comp == 0 ? cx3(j) : (comp == 1 ? cy3(j) : cz3(j)); };
+  base.assign((size_t)N, -1);
+  links.clear();
+  for (int z = 0; z < D; z++)
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        const long long idx = at(x, y, z);
+        const uint32_t f = fl[(size_t)idx];
+        if (f == 0u || (f & (FLAG3_SOLID | FLAG3_INLET))) continue;
+        const bool outlet = (f & FLAG3_OUTLET) != 0u;
+        bool any = false;
+        for (int i = 1; i < Q3; i++) {
+          if (!(f & (1u << i))) continue;
+          if (!any) {
+            base[(size_t)idx] = (int)links.size();
+            any = true;
+          }
+          AdjLink3Host L{};
+          L.e2 = -1;
+          L.a1 = 1.0;
+          L.a2 = 0.0;
+          L.cell = (int)idx;
+          L.solid = -1;
+          const int j = opp3(i);
+          const int sx = x - cx3(i), sy = y - cy3(i), sz = z - cz3(i);
+          const bool outX = sx < 0 || sx >= W, outY = sy < 0 || sy >= H, outZ = sz < 0 || sz >= D;
+          if (outX && outlet) {
+            L.e1 = i * N + at(W - 2, y, z);
+          } else if (outY && outZ) {
+            L.e1 = j * N + idx;
+          } else if (outY || outZ) {
+            int rx = sx, ry = sy, rz = sz, m = mirror_y3(i);
+            if (outY) {
+              ry = y;
+            } else {
+              rz = z;
+              m = mirror_z3(i);
+            }
+            const long long rs = at(rx, ry, rz);
+            if (solid(rs)) {  // a body meets a slip face: bounce-back with force 2 c_j f_j
+              L.e1 = j * N + idx;
+              L.cF = cc(j);
+            } else {
+              L.e1 = m * N + rs;
+            }
+          } else if (outX) {
+            L.e1 = j * N + idx;
+          } else {
+            const long long s = at(sx, sy, sz);
+            if (!solid(s)) {
+              L.e1 = i * N + s;
+            } else {
+              // Bouzidi: q in the arithmetic type, as the step kernel computes it
+              const R dF = (R)sdf[(size_t)idx], dS = (R)sdf[(size_t)s];
+              const R den = std::max(dF - dS, (R)1e-6);
+              const R raw = dF / den;
+              const R q = std::min(std::max(raw, (R)1e-3), R(1));
+              L.e1 = j * N + idx;
+              L.cF = cc(j);
+              L.q = (double)q;
+              L.cell = (int)idx;
+              L.solid = (int)s;
+              const bool free = raw > (R)1e-3 && raw < R(1) && (dF - dS) > (R)1e-6;
+              if (free) {
+                L.dqdF = -(double)dS / ((double)den * (double)den);
+                L.dqdS = (double)dF / ((double)den * (double)den);
+              }
+              if (q < R(0.5)) {
+                const int nx = x + cx3(i), ny = y + cy3(i), nz = z + cz3(i);
+                if (nx >= 0 && nx < W && ny >= 0 && ny < H && nz >= 0 && nz < D && !solid(at(nx, ny, nz))) {
+                  L.a1 = (double)(R(2) * q);
+                  L.e2 = j * N + at(nx, ny, nz);
+                  L.a2 = (double)(R(1) - R(2) * q);
+                  L.qKind = 1;
+                }
+              } else {
+                L.a1 = (double)(R(1) / (R(2) * q));
+                L.e2 = i * N + idx;
+                L.a2 = (double)((R(2) * q - R(1)) / (R(2) * q));
+                L.qKind = 2;
+              }
+            }
+          }
+          links.push_back(L);
+        }
+      }
+}
+
+template <class R>
+void upload_typed(cells::Device& dev, void* d, const std::vector<double>& v) {
+  std::vector<R> t(v.begin(), v.end());
+  if (!t.empty()) dev.h2d(d, t.data(), t.size() * sizeof(R));
+  dev.sync();
+}
+
+void release_adjoint(Cells3D* h) {
+  if (!h->adj) return;
+  Adjoint3D* A = h->adj.get();
+  std::vector<void*> ptrs = {A->endState, A->linkBase, A->le1, A->le2, A->la1, A->la2, A->lcF, A->lq, A->lqk,
+                             A->lamG, A->dqAcc, A->rowElem, A->rowSet, A->rowStart, A->entLink, A->entAlpha,
+                             A->rowPhi, A->lam[0], A->lam[1], A->blockPart, A->counter, A->dudn};
+  for (void* p : A->ck) ptrs.push_back(p);
+  for (void* p : A->ckState) ptrs.push_back(p);
+  for (void* p : A->seg) ptrs.push_back(p);
+  if (!h->dev.fake) h->dev.sync();
+  for (void* p : ptrs)
+    if (p) h->dev.release(p);
+  h->adj.reset();
+}
+
+// Link tables and the transposed element map for the current flags and SDF.
+void build_tables(Cells3D* h, Adjoint3D* A) {
+  cells::Device& dev = h->dev;
+  const long long N = h->N;
+  const int W = h->W, H = h->H, D = h->D;
+  std::vector<uint32_t> fl((size_t)N);
+  std::vector<float> sdf((size_t)N);
+  dev.d2h(fl.data(), h->flags, (size_t)N * 4);
+  dev.d2h(sdf.data(), h->sdf, (size_t)N * 4);
+  dev.sync();
+  std::vector<int> base;
+  if (h->prec == 3)
+    resolve_links<double>(h, fl, sdf, A->component, base, A->hostLinks);
+  else
+    resolve_links<float>(h, fl, sdf, A->component, base, A->hostLinks);
+  const std::vector<AdjLink3Host>& L = A->hostLinks;
+  A->nLinks = (int)L.size();
+  // transposed map: (element, link, alpha) entries, direct force terms, and elements without a
+  // regular reader
+  struct Ent {
+    long long e;
+    int link;  // -1: no regular reader; -2: a force term
+    double alpha;
+  };
+  std::vector<Ent> ents;
+  ents.reserve(L.size() * 3);
+  for (int k = 0; k < A->nLinks; k++) {
+    ents.push_back({L[k].e1, k, L[k].a1});
+    if (L[k].e2 >= 0) ents.push_back({L[k].e2, k, L[k].a2});
+    if (L[k].cF != 0.0) ents.push_back({L[k].e1, -2, L[k].cF});
+  }
+  auto at = [&](int x, int y, int z) { return (long long)x + (long long)W * ((long long)y + (long long)H * z); };
+  for (int z = 0; z < D; z++)
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        const long long c = at(x, y, z);
+        if (fl[(size_t)c] & FLAG3_SOLID) continue;
+        for (int i = 0; i < Q3; i++) {
+          const int rx = x + cx3(i), ry = y + cy3(i), rz = z + cz3(i);
+          bool regular = rx >= 0 && rx < W && ry >= 0 && ry < H && rz >= 0 && rz < D;
+          if (regular) {
+            const uint32_t g = fl[(size_t)at(rx, ry, rz)];
+            regular = !(g & (FLAG3_SOLID | FLAG3_INLET)) && (i == 0 || !(g & (1u << i)));
+          }
+          if (!regular) ents.push_back({i * N + c, -1, 0.0});
+        }
+      }
+  std::stable_sort(ents.begin(), ents.end(), [](const Ent& a, const Ent& b) { return a.e < b.e; });
+  std::vector<long long> rowElem;
+  std::vector<unsigned char> rowSet;
+  std::vector<int> rowStart, entLink;
+  std::vector<double> entAlpha, rowPhi;
+  for (size_t p = 0; p < ents.size();) {
+    const long long e = ents[p].e;
+    unsigned char set = 0;
+    double phi = 0.0;
+    rowElem.push_back(e);
+    rowStart.push_back((int)entLink.size());
+    for (; p < ents.size() && ents[p].e == e; p++) {
+      if (ents[p].link == -1) {
+        set = 1;
+      } else if (ents[p].link == -2) {
+        phi += ents[p].alpha;
+      } else {
+        entLink.push_back(ents[p].link);
+        entAlpha.push_back(ents[p].alpha);
+      }
+    }
+    rowSet.push_back(set);
+    rowPhi.push_back(phi);
+  }
+  rowStart.push_back((int)entLink.size());
+  A->nRows = (int)rowElem.size();
+  const size_t rb = h->prec == 3 ? 8 : 4;
+  auto up_r = [&](void* d, const std::vector<double>& v) {
+    if (h->prec == 3)
+      upload_typed<double>(dev, d, v);
+    else
+      upload_typed<float>(dev, d, v);
+  };
+  const size_t nl = std::max<size_t>(1, L.size());
+  A->linkBase = (int*)dev.alloc((size_t)N * 4, "adjoint link base");
+  dev.h2d(A->linkBase, base.data(), (size_t)N * 4);
+  dev.sync();
+  std::vector<long long> e1(L.size()), e2(L.size());
+  std::vector<double> a1(L.size()), a2(L.size()), cF(L.size()), q(L.size());
+  std::vector<signed char> qk(L.size());
+  for (size_t k = 0; k < L.size(); k++) {
+    e1[k] = L[k].e1;
+    e2[k] = L[k].e2;
+    a1[k] = L[k].a1;
+    a2[k] = L[k].a2;
+    cF[k] = L[k].cF;
+    q[k] = L[k].q;
+    qk[k] = (signed char)L[k].qKind;
+  }
+  A->le1 = (long long*)dev.alloc(nl * 8, "adjoint links");
+  A->le2 = (long long*)dev.alloc(nl * 8, "adjoint links");
+  A->la1 = dev.alloc(nl * rb, "adjoint links");
+  A->la2 = dev.alloc(nl * rb, "adjoint links");
+  A->lcF = dev.alloc(nl * rb, "adjoint links");
+  A->lq = dev.alloc(nl * rb, "adjoint links");
+  A->lqk = (signed char*)dev.alloc(nl, "adjoint links");
+  A->lamG = dev.alloc(nl * rb, "adjoint link values");
+  A->dqAcc = (double*)dev.alloc(nl * 8, "adjoint dJ/dq");
+  if (!L.empty()) {
+    dev.h2d(A->le1, e1.data(), L.size() * 8);
+    dev.h2d(A->le2, e2.data(), L.size() * 8);
+    dev.h2d(A->lqk, qk.data(), L.size());
+    dev.sync();
+    up_r(A->la1, a1);
+    up_r(A->la2, a2);
+    up_r(A->lcF, cF);
+    up_r(A->lq, q);
+  }
+  const size_t nr = std::max<size_t>(1, rowElem.size());
+  const size_t ne = std::max<size_t>(1, entLink.size());
+  A->rowElem = (long long*)dev.alloc(nr * 8, "adjoint rows");
+  A->rowSet = (unsigned char*)dev.alloc(nr, "adjoint rows");
+  A->rowStart = (int*)dev.alloc((nr + 1) * 4, "adjoint rows");
+  A->rowPhi = dev.alloc(nr * rb, "adjoint rows");
+  A->entLink = (int*)dev.alloc(ne * 4, "adjoint rows");
+  A->entAlpha = dev.alloc(ne * rb, "adjoint rows");
+  if (!rowElem.empty()) {
+    dev.h2d(A->rowElem, rowElem.data(), rowElem.size() * 8);
+    dev.h2d(A->rowSet, rowSet.data(), rowSet.size());
+    dev.h2d(A->rowStart, rowStart.data(), rowStart.size() * 4);
+    if (!entLink.empty()) dev.h2d(A->entLink, entLink.data(), entLink.size() * 4);
+    dev.sync();
+    up_r(A->rowPhi, rowPhi);
+    if (!entAlpha.empty()) up_r(A->entAlpha, entAlpha);
+  }
+}
+
+}  // namespace
+
+// ---------------- C ABI ----------------
+
+#define ADJ_TRY(h) try {
+#define ADJ_CATCH(h)                                                         \
+  }                                                                          \
+  catch (const AllocError& e) {                                              \
+    release_adjoint(h);                                                      \
+    (h)->lastError = std::string("Solver3D allocation failed: ") + e.what(); \
+    return CELLS_E_ALLOC;                                                    \
+  }                                                                          \
+  catch (const Error& e) {                                                   \
+    (h)->lastError = e.what();                                               \
+    return e.status;                                                         \
+  }                                                                          \
+  catch (const std::exception& e) {                                          \
+    (h)->lastError = e.what();                                               \
+    return CELLS_E_INVALID;                                                  \
+  }                                                                          \
+  return CELLS_OK;
+
+extern "C" {
+
+int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* objective) {
+  if (!h || !spec) return CELLS_E_INVALID;
+  ADJ_TRY(h)
+  if (h->dev.fake) throw Error(CELLS_E_INVALID, "the adjoint needs a CUDA device");
+  if (h->prec != CELLS_FP32 && h->prec != CELLS_FP64)
+    throw Error(CELLS_E_PRECISION_UNSUPPORTED, "the adjoint runs with FP32 or FP64 storage");
+  if (h->cfg.smagorinsky != 0.0) throw Error(CELLS_E_INVALID, "the adjoint supports smagorinsky = 0 only");
+  if (spec->steps <= 0 || spec->checkpoint_every <= 0) throw Error(CELLS_E_INVALID, "steps and checkpoint_every must be positive");
+  if (spec->component < 0 || spec->component > 2) throw Error(CELLS_E_INVALID, "component must be 0, 1 or 2");
+  const int64_t s0 = h->step;
+  if (spec->window_begin > spec->window_end || spec->window_begin <= s0 || spec->window_end > s0 + spec->steps)
+    throw Error(CELLS_E_INVALID, "the objective window must lie within the recorded steps");
+  const int64_t nWin = spec->window_end - spec->window_begin + 1;
+  if (nWin > HISTORY_LEN) throw Error(CELLS_E_INVALID, "the objective window exceeds the 8192-sample force ring");
+  release_adjoint(h);
+  h->adj.reset(new Adjoint3D());
+  Adjoint3D* A = h->adj.get();
+  A->s0 = s0;
+  A->steps = spec->steps;
+  A->w0 = spec->window_begin;
+  A->w1 = spec->window_end;
+  A->K = spec->checkpoint_every;
+  A->component = spec->component;
+  A->scale = spec->scale;
+  A->parity0 = h->parity;
+  cells::Device& dev = h->dev;
+  const size_t fBytes = 19ull * h->bpp * (size_t)h->N;
+  const int64_t nSeg = (A->steps + A->K - 1) / A->K;
+  const int segBufs = (int)std::min<int64_t>(A->K, A->steps) - 1;
+  const size_t need = (size_t)(nSeg + segBufs + 2) * fBytes + (size_t)h->N * 16;
+  if (need > dev.free_bytes())
+    throw AllocError("the adjoint's checkpoints need " + std::to_string(need) + " bytes; the device has " +
+                     std::to_string(dev.free_bytes()) + " free");
+  build_tables(h, A);
+  for (int64_t k = 0; k < nSeg; k++) {
+    A->ck.push_back(dev.alloc(fBytes, "adjoint checkpoint"));
+    A->ckState.push_back(dev.alloc(sizeof(DevState3), "adjoint checkpoint"));
+  }
+  for (int k = 0; k < segBufs; k++) A->seg.push_back(dev.alloc(fBytes, "adjoint segment"));
+  A->endState = dev.alloc(sizeof(DevState3), "adjoint end state");
+  A->lam[0] = dev.alloc(fBytes, "adjoint state");
+  A->lam[1] = dev.alloc(fBytes, "adjoint state");
+  A->nBlocks = (int)((h->N + kAdjThreads - 1) / kAdjThreads);
+  A->blockPart = (double*)dev.alloc((size_t)A->nBlocks * 8, "adjoint partials");
+  A->counter = (unsigned*)dev.alloc(64, "adjoint counter");
+  A->dudn = (double*)dev.alloc((size_t)A->steps * 8, "adjoint du");
+  // the recorded run: a checkpoint at the start of every segment, force samples in the window
+  const uint64_t written0 = h->forceSamplesRead + h->forceSteps.size();
+  A->uStep.resize((size_t)A->steps);
+  A->rampStep.resize((size_t)A->steps);
+  for (int64_t n = 0; n < A->steps; n++) {
+    const int64_t s = s0 + n;
+    A->uStep[(size_t)n] = h->uin_at(s);
+    A->rampStep[(size_t)n] = h->rampKind ? (h->rampTarget != 0.0 ? h->ramp_speed(s) / h->rampTarget : 0.0) : 1.0;
+    if (n % A->K == 0) {
+      const int64_t k = n / A->K;
+      check_cuda(cudaMemcpyAsync(A->ck[(size_t)k], h->f[h->parity], fBytes, cudaMemcpyDeviceToDevice, dev.stream),
+                 "checkpoint copy");
+      check_cuda(cudaMemcpyAsync(A->ckState[(size_t)k], h->st, sizeof(DevState3), cudaMemcpyDeviceToDevice,
+                                 dev.stream),
+                 "checkpoint copy");
+    }
+    const int64_t label = s + 1;
+    const bool sample = label >= A->w0 && label <= A->w1;
+    h->enqueue_step_between(h->f[h->parity], h->f[h->parity ^ 1], h->parity, sample);
+    dev.launches++;
+    h->parity ^= 1;
+    h->step++;
+    if (sample) h->forceSteps.push_back((uint32_t)h->step);
+  }
+  check_cuda(cudaMemcpyAsync(A->endState, h->st, sizeof(DevState3), cudaMemcpyDeviceToDevice, dev.stream),
+             "end state copy");
+  // the objective from the window's samples (ring slots written0 .. written0 + nWin - 1)
+  std::vector<double4> hist((size_t)nWin);
+  size_t got = 0;
+  for (uint64_t k = written0; k < written0 + (uint64_t)nWin;) {
+    const size_t r = (size_t)(k % HISTORY_LEN);
+    const size_t run = (size_t)std::min<uint64_t>(written0 + nWin - k, (uint64_t)(HISTORY_LEN - r));
+    dev.d2h(hist.data() + got, h->history + r, run * sizeof(double4));
+    got += run;
+    k += run;
+  }
+  dev.sync();
+  double sum = 0.0;
+  for (const double4& v : hist) sum += A->component == 0 ? v.x : (A->component == 1 ? v.y : v.z);
+  A->objective = A->scale * sum / (double)nWin;
+  A->endStep = h->step;
+  A->argGen = h->argGen;
+  if (objective) *objective = A->objective;
+  ADJ_CATCH(h)
+}
+
+int cells3d_adjoint_backward(Cells3D* h, const void* terminal_adjoint, double* dJ_dsdf, double* dJ_du_in,
+                             void* adjoint_out) {
+  if (!h) return CELLS_E_INVALID;
+  ADJ_TRY(h)
+  Adjoint3D* A = h->adj.get();
+  if (!A) throw Error(CELLS_E_INVALID, "adjoint_backward needs a recorded adjoint_forward");
+  if (h->step != A->endStep || h->argGen != A->argGen)
+    throw Error(CELLS_E_INVALID, "the solver changed after adjoint_forward: record the run again");
+  cells::Device& dev = h->dev;
+  const long long N = h->N;
+  const size_t fBytes = 19ull * h->bpp * (size_t)N;
+  dev.memset0(A->lam[0], fBytes);
+  dev.memset0(A->lam[1], fBytes);
+  dev.memset0(A->dqAcc, (size_t)std::max(1, A->nLinks) * 8);
+  dev.memset0(A->dudn, (size_t)A->steps * 8);
+  dev.memset0(A->counter, 4);
+  int cur = 0;
+  if (terminal_adjoint) {
+    dev.h2d(A->lam[0], terminal_adjoint, fBytes);
+    dev.sync();
+  }
+  const int64_t nWin = A->w1 - A->w0 + 1;
+  const int64_t nSeg = (A->steps + A->K - 1) / A->K;
+  AdjLaunch3 a;
+  std::memset(&a, 0, sizeof(a));
+  a.flags = h->flags;
+  a.xTab = h->xTab;
+  a.linkBase = A->linkBase;
+  a.le1 = A->le1;
+  a.le2 = A->le2;
+  a.la1 = A->la1;
+  a.la2 = A->la2;
+  a.lcF = A->lcF;
+  a.lq = A->lq;
+  a.lqk = A->lqk;
+  a.lamG = A->lamG;
+  a.dqAcc = A->dqAcc;
+  a.blockPart = A->blockPart;
+  a.counter = A->counter;
+  a.N = N;
+  a.W = h->W;
+  a.H = h->H;
+  a.D = h->D;
+  a.nRows = A->nRows;
+  a.rowElem = A->rowElem;
+  a.rowSet = A->rowSet;
+  a.rowStart = A->rowStart;
+  a.entLink = A->entLink;
+  a.entAlpha = A->entAlpha;
+  a.rowPhi = A->rowPhi;
+  for (int64_t sgi = nSeg - 1; sgi >= 0; sgi--) {
+    const int64_t n0 = sgi * A->K;
+    const int len = (int)std::min<int64_t>(A->K, A->steps - n0);
+    // recompute the segment's states from its checkpoint (no force sampling)
+    check_cuda(cudaMemcpyAsync(h->st, A->ckState[(size_t)sgi], sizeof(DevState3), cudaMemcpyDeviceToDevice,
+                               dev.stream),
+               "checkpoint restore");
+    auto state = [&](int t) -> void* { return t == 0 ? A->ck[(size_t)sgi] : A->seg[(size_t)(t - 1)]; };
+    const int par0 = (int)((A->parity0 + n0) & 1);
+    for (int t = 0; t + 1 < len; t++) {
+      h->enqueue_step_between(state(t), state(t + 1), par0 ^ (t & 1), false);
+      dev.launches++;
+    }
+    for (int t = len - 1; t >= 0; t--) {
+      const int64_t n = n0 + t;
+      const int64_t label = A->s0 + n + 1;
+      a.f = state(t);
+      a.lamNext = A->lam[cur];
+      a.lamOut = A->lam[cur ^ 1];
+      a.u = A->uStep[(size_t)n];
+      a.w = (label >= A->w0 && label <= A->w1) ? A->scale / (double)nWin : 0.0;
+      a.dudOut = A->dudn + n;
+      check_cuda(launch_adjoint_step3(h->prec, a, dev.stream), "adjoint step kernel");
+      dev.launches += 2;
+      cur ^= 1;
+    }
+  }
+  check_cuda(cudaMemcpyAsync(h->st, A->endState, sizeof(DevState3), cudaMemcpyDeviceToDevice, dev.stream),
+             "end state restore");
+  if (adjoint_out) dev.d2h(adjoint_out, A->lam[cur], fBytes);
+  std::vector<double> dq((size_t)std::max(1, A->nLinks)), dudn((size_t)A->steps);
+  dev.d2h(dq.data(), A->dqAcc, dq.size() * 8);
+  dev.d2h(dudn.data(), A->dudn, dudn.size() * 8);
+  dev.sync();
+  if (dJ_dsdf) {
+    std::fill(dJ_dsdf, dJ_dsdf + N, 0.0);
+    for (int k = 0; k < A->nLinks; k++) {
+      const AdjLink3Host& L = A->hostLinks[(size_t)k];
+      if (L.qKind == 0 || L.solid < 0) continue;
+      dJ_dsdf[L.cell] += dq[(size_t)k] * L.dqdF;
+      dJ_dsdf[L.solid] += dq[(size_t)k] * L.dqdS;
+    }
+  }
+  if (dJ_du_in) {
+    double s = 0.0;
+    for (int64_t n = 0; n < A->steps; n++) s += dudn[(size_t)n] * A->rampStep[(size_t)n];
+    *dJ_du_in = s;
+  }
+  ADJ_CATCH(h)
+}
+
+int cells3d_adjoint_release(Cells3D* h) {
+  if (!h) return CELLS_E_INVALID;
+  ADJ_TRY(h)
+  release_adjoint(h);
+  ADJ_CATCH(h)
+}
+
+}  // extern "C"

@@ -207,6 +207,32 @@ class Solver3D:
         check(lib().cells3d_read_flags(self._h, out.ctypes.data, out.size), self._h)
         return out
 
+    # ------------------------------------------------------------------ discrete adjoint
+    def adjointForward(self, steps: int, windowBegin: int, windowEnd: int, checkpointEvery: int = 100,
+                       component: int = 0, scale: float = 1.0) -> float:
+        """Steps `steps` steps with checkpoints and returns J = scale * mean force component over
+        the window of step labels [windowBegin, windowEnd] (absolute step counts)."""
+        spec = _lib.Cells3DAdjointSpec(steps, windowBegin, windowEnd, checkpointEvery, component, scale)
+        j = C.c_double()
+        check(lib().cells3d_adjoint_forward(self._h, C.byref(spec), C.byref(j)), self._h)
+        return j.value
+
+    def adjointBackward(self, terminal: Optional[np.ndarray] = None, wantAdjoint: bool = False) -> dict:
+        """The backward sweep of the recorded run: dJ/dsdf (N float64), dJ/du_in, and optionally
+        the adjoint of the initial populations (seeded with `terminal` at the final state)."""
+        dsdf = np.zeros(self.N, dtype=np.float64)
+        du = C.c_double()
+        t = None
+        if terminal is not None:
+            t = np.ascontiguousarray(terminal, dtype=self._pop_dtype())
+        out = np.empty(19 * self.N, dtype=self._pop_dtype()) if wantAdjoint else None
+        check(lib().cells3d_adjoint_backward(self._h, None if t is None else t.ctypes.data, dsdf.ctypes.data,
+                                             C.byref(du), None if out is None else out.ctypes.data), self._h)
+        return {"dsdf": dsdf, "du": du.value, "adjoint": out}
+
+    def adjointRelease(self) -> None:
+        check(lib().cells3d_adjoint_release(self._h), self._h)
+
     # ------------------------------------------------------------------ timing
     def timerStart(self) -> None:
         check(lib().cells3d_timer_start(self._h), self._h)

@@ -188,6 +188,37 @@ int cells3d_read_flags(Cells3D* h, uint32_t* out, size_t n);
 int cells3d_mass_noalloc(const void* populations, const uint32_t* flags, int64_t n_cells, int32_t precision,
                          double* out_device, void* stream);
 
+/* ---------------- discrete adjoint (no counterpart in the reference) ----------------
+ * The forward/backward pair of a differentiable run: adjoint_forward steps the solver `steps`
+ * steps from its current state (exactly like cells3d_step, plus a checkpoint of the populations
+ * every checkpoint_every steps) and returns J = scale * mean over the window of the force
+ * component; adjoint_backward then sweeps the discrete adjoint of those steps back to the start,
+ * recomputing each segment of checkpoint_every steps from its checkpoint, and returns
+ *   dJ_dsdf[N]  dJ/d(SDF value of every node): the shape gradient through the Bouzidi link
+ *               fractions q(sdf) (cells whose solidity would flip are a discrete change and have
+ *               no derivative);
+ *   dJ_du_in    dJ/d(inflow speed): the ramp target when a device ramp is set, else the inlet speed,
+ *               with `scale` held fixed (a caller whose scale is 2/(u^2 A) adds -2 J / u);
+ *   adjoint_out the adjoint of the initial populations (19 N values of the storage type), for
+ *               adjoint tests; terminal_adjoint (or NULL = 0) seeds the adjoint of the final state.
+ * FP32 or FP64 storage, Smagorinsky off. Force samples of the window go to the force ring as usual
+ * (other steps of the recorded run are not sampled). Any change to the solver after the forward
+ * run (parameters, SDF, steps) invalidates it. */
+typedef struct {
+  int64_t steps;             /* steps of the recorded run */
+  int64_t window_begin;      /* first and last step label (the step count after the step) */
+  int64_t window_end;        /*   averaged by the objective; inside the recorded run */
+  int32_t checkpoint_every;  /* K: one checkpoint of the populations every K steps */
+  int32_t component;         /* force component: 0 x (drag), 1 y, 2 z */
+  double scale;              /* J = scale * mean of the force component over the window */
+} Cells3DAdjointSpec;
+
+int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* objective);
+int cells3d_adjoint_backward(Cells3D* h, const void* terminal_adjoint, double* dJ_dsdf, double* dJ_du_in,
+                             void* adjoint_out);
+/* Frees the recorded run's checkpoints and tables. */
+int cells3d_adjoint_release(Cells3D* h);
+
 /* ---------------- timing (CUDA events on the handle's stream) ---------------- */
 int cells3d_timer_start(Cells3D* h);
 int cells3d_timer_stop(Cells3D* h, float* ms);

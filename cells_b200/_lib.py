@@ -135,6 +135,9 @@ def lib() -> C.CDLL:
         "cells3d_adjoint_forward": (I, [P, C.POINTER(Cells3DAdjointSpec), C.POINTER(D)]),
         "cells3d_adjoint_backward": (I, [P, P, P, C.POINTER(D), P]),
         "cells3d_adjoint_release": (I, [P]),
+        "cells3d_state_size": (I, [P, C.POINTER(SZ)]),
+        "cells3d_save_state": (I, [P, P, SZ]),
+        "cells3d_load_state": (I, [P, P, SZ]),
         # D2Q9 (Solver, src/solver.ts) and batches of 2D tunnels
         "cells2d_config_default": (None, [C.POINTER(Cells2DConfig)]),
         "cells2d_create": (I, [C.POINTER(Cells2DConfig), C.POINTER(P)]),

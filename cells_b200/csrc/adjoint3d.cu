@@ -139,121 +139,180 @@ __device__ __forceinline__ void outlet_adjoint3(const R g[Q3], const R lp[Q3], R
   for (int i = 0; i < Q3; i++) lg[i] = rhoB + R(cx3(i)) * jxB + R(cy3(i)) * jyB + R(cz3(i)) * jzB;
 }
 
+// The recorded step this adjoint step undoes: the segment's first step (device memory, written
+// before the segment's kernels run, so one captured graph serves every segment) plus the kernel's
+// position t within the segment.
+__device__ __forceinline__ int adj_step(const AdjLaunch3& a) { return __ldg(a.n0Dev) + a.t; }
+
+// The block's f64 sum of dJ/du_n into part[slot] (the rows kernel sums the slots in order).
+__device__ __forceinline__ void block_du_partial(double du, double* part, int slot, double* red, int tid) {
+  for (int o = 16; o > 0; o >>= 1) du += __shfl_down_sync(0xffffffffu, du, o);
+  if ((tid & 31) == 0) red[tid >> 5] = du;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0.0;
+    for (int k = 0; k < kAdjThreads / 32; k++) s += red[k];
+    part[slot] = s;
+  }
+}
+
 template <class R>
 __global__ void __launch_bounds__(kAdjThreads) adj_cells3_kernel(AdjLaunch3 a) {
   __shared__ double red[kAdjThreads / 32];
-  __shared__ bool last;
-  const long long N = a.N;
-  const long long idx = (long long)blockIdx.x * kAdjThreads + threadIdx.x;
+  // a tile of x-rows per block (no division per cell); 32-bit element indices (19 N < 2^31)
+  const int W = a.W, H = a.H;
+  const int N = (int)a.N;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   const R* __restrict__ f = (const R*)a.f;
   const R* __restrict__ lamNext = (const R*)a.lamNext;
   R* __restrict__ lamOut = (R*)a.lamOut;
   double du = 0.0;
-  if (idx < N) {
+  const int idx = x + W * (y + H * (int)blockIdx.z);
+  const uint32_t fl = (x < W && y < H) ? __ldg(&a.flags[idx]) : FLAG3_SOLID;
+  if (fl == 0u) {
+    // interior cell: plain pulls, the collision's transposed Jacobian, plain pushes
+    R g[Q3], lp[Q3], lg[Q3];
+#pragma unroll
+    for (int i = 0; i < Q3; i++) {
+      const int o = i * N + idx;
+      lp[i] = __ldg(&lamNext[o]);
+      g[i] = __ldg(&f[o - (int)off3(i, W, H)]);
+    }
+    const R* xt = (const R*)a.xTab + 4 * x;
+    R dut = R(0);
+    collide_adjoint3<R>(g, lp, xt[0], xt[1], xt[2], (R)__ldg(&a.uDev[adj_step(a)]), lg, dut);
+    du = (double)dut;
+#pragma unroll
+    for (int i = 0; i < Q3; i++) lamOut[i * N + idx - (int)off3(i, W, H)] = lg[i];
+  }
+  // flagged fluid cells (faces, inlet, outlet, body) are done by adj_slow3_kernel
+  block_du_partial(du, a.blockPart, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), red, tid);
+}
+
+// The flagged fluid cells (faces, inlet, outlet, body), kSlowCells per block in three phases so
+// that their many independent loads are in flight together: (cell, direction) items pull through
+// the cells' records into shared memory; one thread per cell applies the transposed Jacobian of its
+// collision (or of the outlet equilibrium; the inlet only feeds dJ/du_n); (cell, direction) items
+// push the plain pulls' adjoints and store the links' adjoints (with dJ/dq of Bouzidi links).
+constexpr int kSlowCells = 32;
+
+template <class R>
+__global__ void __launch_bounds__(kAdjThreads) adj_slow3_kernel(AdjLaunch3 a) {
+  __shared__ double red[kAdjThreads / 32];
+  __shared__ R sg[Q3][kSlowCells + 1];
+  __shared__ R slp[Q3][kSlowCells + 1];
+  __shared__ R slg[Q3][kSlowCells + 1];
+  __shared__ uint32_t sfl[kSlowCells];
+  const int N = (int)a.N;
+  const int n = a.nSlow;
+  const int tid = threadIdx.x;
+  const int c0 = blockIdx.x * kSlowCells;
+  const R* __restrict__ f = (const R*)a.f;
+  const R* __restrict__ lamNext = (const R*)a.lamNext;
+  R* __restrict__ lamOut = (R*)a.lamOut;
+  const R* sA1 = (const R*)a.sA1;
+  const R* sA2 = (const R*)a.sA2;
+  for (int it = tid; it < Q3 * kSlowCells; it += kAdjThreads) {
+    const int c = it % kSlowCells, i = it / kSlowCells, s = c0 + c;
+    if (s >= n) continue;
+    const int idx = a.slowCells[s];
+    const int r = i * n + s;
+    slp[i][c] = lamNext[i * N + idx];
+    const int e = a.sE1[r];
+    if (e >= 0) {  // one source with coefficient 1: plain pulls, copies, mirrors, bounce-back
+      sg[i][c] = f[e];
+    } else {       // Bouzidi interpolation: two sources
+      sg[i][c] = sA1[r] * f[e & 0x7fffffff] + sA2[r] * f[a.sE2[r]];
+    }
+  }
+  __syncthreads();
+  double du = 0.0;
+  if (tid < kSlowCells && c0 + tid < n) {
+    const int idx = a.slowCells[c0 + tid];
     const uint32_t fl = a.flags[idx];
-    if (!(fl & FLAG3_SOLID)) {
-      R lp[Q3];
+    sfl[tid] = fl;
+    R g[Q3], lp[Q3], lg[Q3];
 #pragma unroll
-      for (int i = 0; i < Q3; i++) lp[i] = lamNext[i * N + idx];
-      const R u = (R)a.u;
-      if (fl & FLAG3_INLET) {
-        // f' = feq(1, u, 0, 0): d/du = w_i (3 c_ix + 9 c_ix^2 u - 3 u)
-        R s = R(0);
+    for (int i = 0; i < Q3; i++) {
+      g[i] = sg[i][tid];
+      lp[i] = slp[i][tid];
+    }
+    const R u = (R)__ldg(&a.uDev[adj_step(a)]);
+    if (fl & FLAG3_INLET) {
+      // f' = feq(1, u, 0, 0): d/du = w_i (3 c_ix + 9 c_ix^2 u - 3 u); the inlet reads nothing
+      R sum = R(0);
 #pragma unroll
-        for (int i = 0; i < Q3; i++) {
-          const R c = R(cx3(i));
-          s += lp[i] * w3<R>(i) * (R(3) * c + R(9) * c * c * u - R(3) * u);
-        }
-        du = (double)s;
-      } else {
-        const int W = a.W, H = a.H;
-        const int base = fl ? a.linkBase[idx] : -1;
-        const R* la1 = (const R*)a.la1;
-        const R* la2 = (const R*)a.la2;
-        R g[Q3];
-        int rank = 0;
+      for (int i = 0; i < Q3; i++) {
+        const R c = R(cx3(i));
+        sum += lp[i] * w3<R>(i) * (R(3) * c + R(9) * c * c * u - R(3) * u);
+        lg[i] = R(0);
+      }
+      du = (double)sum;
+    } else if (fl & FLAG3_OUTLET) {
+      outlet_adjoint3<R>(g, lp, lg);
+    } else {
+      const R* xt = (const R*)a.xTab + 4 * (idx % a.W);
+      R dut = R(0);
+      collide_adjoint3<R>(g, lp, xt[0], xt[1], xt[2], u, lg, dut);
+      du = (double)dut;
+    }
 #pragma unroll
-        for (int i = 0; i < Q3; i++) {
-          if (i == 0 || !(fl & (1u << i))) {
-            g[i] = f[i * N + idx - off3(i, W, H)];
-          } else {
-            const int k = base + rank++;
-            const long long e2 = a.le2[k];
-            g[i] = la1[k] * f[a.le1[k]] + (e2 >= 0 ? la2[k] * f[e2] : R(0));
-          }
-        }
-        R lg[Q3];
-        if (fl & FLAG3_OUTLET) {
-          outlet_adjoint3<R>(g, lp, lg);
-        } else {
-          const int x = (int)(idx % W);
-          const R* xt = (const R*)a.xTab + 4 * x;
-          R dut = R(0);
-          collide_adjoint3<R>(g, lp, xt[0], xt[1], xt[2], u, lg, dut);
-          du = (double)dut;
-        }
-        const R* lcF = (const R*)a.lcF;
-        const R* lq = (const R*)a.lq;
-        R* lamG = (R*)a.lamG;
-        const R w = (R)a.w;
-        rank = 0;
-#pragma unroll
-        for (int i = 0; i < Q3; i++) {
-          if (i == 0 || !(fl & (1u << i))) {
-            lamOut[i * N + idx - off3(i, W, H)] = lg[i];
-          } else {
-            const int k = base + rank++;
-            lamG[k] = lg[i];
-            const int qk = a.lqk[k];
-            if (qk) {
-              const R fj = f[a.le1[k]], f2 = f[a.le2[k]], q = lq[k];
-              const R dgdq = qk == 1 ? R(2) * (fj - f2) : (f2 - fj) / (R(2) * q * q);
-              a.dqAcc[k] += (double)((lg[i] + w * lcF[k]) * dgdq);
-            }
-          }
-        }
+    for (int i = 0; i < Q3; i++) slg[i][tid] = lg[i];
+  }
+  __syncthreads();
+  const R* lcF = (const R*)a.lcF;
+  const R* lq = (const R*)a.lq;
+  R* lamG = (R*)a.lamG;
+  const R w = (R)__ldg(&a.wDev[adj_step(a)]);
+  for (int it = tid; it < Q3 * kSlowCells; it += kAdjThreads) {
+    const int c = it % kSlowCells, i = it / kSlowCells, s = c0 + c;
+    if (s >= n || (sfl[c] & FLAG3_INLET)) continue;
+    const R v = slg[i][c];
+    const int t = a.sTgt[i * n + s];
+    if (t >= 0) {  // a plain pull: the element's only regular reader
+      lamOut[t] = v;
+    } else {       // a link: its adjoint, and dJ/dq of a Bouzidi link
+      const int k = -t - 1;
+      lamG[k] = v;
+      const int qk = a.lqk[k];
+      if (qk) {
+        const R fj = f[a.le1[k]], f2 = f[a.le2[k]], q = lq[k];
+        const R dgdq = qk == 1 ? R(2) * (fj - f2) : (f2 - fj) / (R(2) * q * q);
+        a.dqAcc[k] += (double)((v + w * lcF[k]) * dgdq);
       }
     }
   }
-  // dJ/du_n: block sums in f64, then the last block sums the partials in block order
-  for (int o = 16; o > 0; o >>= 1) du += __shfl_down_sync(0xffffffffu, du, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = du;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int k = 0; k < kAdjThreads / 32; k++) s += red[k];
-    a.blockPart[blockIdx.x] = s;
-    __threadfence();
-    last = atomicAdd(a.counter, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  double s = 0.0;
-  for (unsigned k = threadIdx.x; k < gridDim.x; k += kAdjThreads) s += __ldcg(&a.blockPart[k]);
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int k = 0; k < kAdjThreads / 32; k++) t += red[k];
-    *a.dudOut = t;
-    *a.counter = 0u;
-  }
+  block_du_partial(du, a.blockPart, a.nCellBlocks + (int)blockIdx.x, red, tid);
 }
 
 // Elements with an irregular reader or no regular reader: lambda^n[e] (= 0 when no regular reader
 // wrote it) plus each link's adjoint times its coefficient, plus the direct force terms.
 template <class R>
 __global__ void __launch_bounds__(256) adj_rows3_kernel(AdjLaunch3 a) {
+  if (blockIdx.x == gridDim.x - 1) {
+    // the extra last block: dJ/du_n = the cell kernel's block sums, strided per thread, then in order
+    __shared__ double red[8];
+    double s = 0.0;
+    for (int k = threadIdx.x; k < a.nParts; k += 256) s += a.blockPart[k];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < 8; k++) t += red[k];
+      a.dudn[adj_step(a)] = t;
+    }
+    return;
+  }
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= a.nRows) return;
   R* lamOut = (R*)a.lamOut;
   const R* lamG = (const R*)a.lamG;
   const R* lcF = (const R*)a.lcF;
   const R* alpha = (const R*)a.entAlpha;
-  const R w = (R)a.w;
+  const R w = (R)__ldg(&a.wDev[adj_step(a)]);
   const long long e = a.rowElem[r];
   R v = a.rowSet[r] ? R(0) : lamOut[e];
   for (int k = a.rowStart[r]; k < a.rowStart[r + 1]; k++) {
@@ -265,21 +324,36 @@ __global__ void __launch_bounds__(256) adj_rows3_kernel(AdjLaunch3 a) {
 }
 
 template <class R>
-cudaError_t launch_adjoint_step3_t(const AdjLaunch3& a, cudaStream_t s) {
-  const unsigned blocks = (unsigned)((a.N + kAdjThreads - 1) / kAdjThreads);
-  adj_cells3_kernel<R><<<blocks, kAdjThreads, 0, s>>>(a);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess || a.nRows == 0) return e;
-  adj_rows3_kernel<R><<<(unsigned)((a.nRows + 255) / 256), 256, 0, s>>>(a);
+cudaError_t launch_adjoint_step3_t(const AdjLaunch3& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
+                                   cudaEvent_t join) {
+  const dim3 block(a.tileX, kAdjThreads / a.tileX);
+  const dim3 grid((unsigned)((a.W + block.x - 1) / block.x), (unsigned)((a.H + block.y - 1) / block.y),
+                  (unsigned)a.D);
+  if ((long long)grid.x * grid.y * grid.z != a.nCellBlocks) return cudaErrorInvalidValue;
+  const int slowBlocks = (a.nSlow + kSlowCells - 1) / kSlowCells;
+  if (a.nCellBlocks + slowBlocks != a.nParts) return cudaErrorInvalidValue;
+  cudaError_t e;
+  if (slowBlocks > 0) {  // the flagged cells on the side stream, beside the interior cells
+    if ((e = cudaEventRecord(fork, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(side, fork, 0)) != cudaSuccess) return e;
+    adj_slow3_kernel<R><<<slowBlocks, kAdjThreads, 0, side>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(join, side)) != cudaSuccess) return e;
+  }
+  adj_cells3_kernel<R><<<grid, block, 0, s>>>(a);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (slowBlocks > 0 && (e = cudaStreamWaitEvent(s, join, 0)) != cudaSuccess) return e;
+  adj_rows3_kernel<R><<<(unsigned)((a.nRows + 255) / 256) + 1, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
 }  // namespace
 
 namespace cells {
-cudaError_t launch_adjoint_step3(int precision, const AdjLaunch3& a, cudaStream_t s) {
-  if (precision == 0) return launch_adjoint_step3_t<float>(a, s);
-  if (precision == 3) return launch_adjoint_step3_t<double>(a, s);
+cudaError_t launch_adjoint_step3(int precision, const AdjLaunch3& a, cudaStream_t s, cudaStream_t side,
+                                 cudaEvent_t fork, cudaEvent_t join) {
+  if (precision == 0) return launch_adjoint_step3_t<float>(a, s, side, fork, join);
+  if (precision == 3) return launch_adjoint_step3_t<double>(a, s, side, fork, join);
   return cudaErrorInvalidValue;
 }
 }  // namespace cells
@@ -395,11 +469,28 @@ void release_adjoint(Cells3D* h) {
   Adjoint3D* A = h->adj.get();
   std::vector<void*> ptrs = {A->endState, A->linkBase, A->le1, A->le2, A->la1, A->la2, A->lcF, A->lq, A->lqk,
                              A->lamG, A->dqAcc, A->rowElem, A->rowSet, A->rowStart, A->entLink, A->entAlpha,
-                             A->rowPhi, A->lam[0], A->lam[1], A->blockPart, A->counter, A->dudn};
+                             A->rowPhi, A->lam[0], A->lam[1], A->blockPart, A->counter, A->dudn,
+                             A->slowCells, A->sE1, A->sE2, A->sTgt, A->sA1, A->sA2};
   for (void* p : A->ck) ptrs.push_back(p);
   for (void* p : A->ckState) ptrs.push_back(p);
-  for (void* p : A->seg) ptrs.push_back(p);
+  for (int k = 0; k < 2; k++)
+    for (void* p : A->seg[k]) ptrs.push_back(p);
+  ptrs.push_back(A->uDev);
+  ptrs.push_back(A->wDev);
+  ptrs.push_back(A->n0Dev);
   if (!h->dev.fake) h->dev.sync();
+  if (A->side) cudaStreamSynchronize(A->side);
+  if (A->side2) cudaStreamSynchronize(A->side2);
+  for (auto& row : A->segGraph)
+    for (auto& g : row)
+      if (g) cudaGraphExecDestroy(g);
+  if (A->fork2) cudaEventDestroy(A->fork2);
+  if (A->join2) cudaEventDestroy(A->join2);
+  if (A->side2) cudaStreamDestroy(A->side2);
+  if (A->fork) cudaEventDestroy(A->fork);
+  if (A->join) cudaEventDestroy(A->join);
+  if (A->side) cudaStreamDestroy(A->side);
+  if (A->n0Host) h->dev.free_host_pinned(A->n0Host);
   for (void* p : ptrs)
     if (p) h->dev.release(p);
   h->adj.reset();
@@ -489,6 +580,68 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
   A->linkBase = (int*)dev.alloc((size_t)N * 4, "adjoint link base");
   dev.h2d(A->linkBase, base.data(), (size_t)N * 4);
   dev.sync();
+  std::vector<int> slow;
+  for (long long c = 0; c < N; c++) {
+    const uint32_t v = fl[(size_t)c];
+    if (v != 0u && !(v & FLAG3_SOLID)) slow.push_back((int)c);
+  }
+  A->nSlow = (int)slow.size();
+  A->slowCells = (int*)dev.alloc(std::max<size_t>(1, slow.size()) * 4, "adjoint flagged cells");
+  if (!slow.empty()) {
+    dev.h2d(A->slowCells, slow.data(), slow.size() * 4);
+    dev.sync();
+  }
+  // per flagged cell and direction, [i][cell]: the pull's sources and coefficients, and where its
+  // adjoint goes (an element index, or -(link + 1))
+  const size_t ns = slow.size();
+  std::vector<int> sE1(19 * ns, 0), sE2(19 * ns, 0), sTgt(19 * ns, 0);
+  std::vector<double> sA1(19 * ns, 0.0), sA2(19 * ns, 0.0);
+  for (size_t c = 0; c < ns; c++) {
+    const int idx = slow[c];
+    const uint32_t v = fl[(size_t)idx];
+    if (v & FLAG3_INLET) continue;  // the inlet reads nothing (and has no link records)
+    const int bse = base[(size_t)idx];
+    int rank = 0;
+    for (int i = 0; i < Q3; i++) {
+      const size_t r = (size_t)i * ns + c;
+      if (i == 0 || !(v & (1u << i))) {
+        const int e = (int)(i * N + idx - off3(i, W, H));
+        sE1[r] = sE2[r] = sTgt[r] = e;
+        sA1[r] = 1.0;
+      } else {
+        const int k = bse + rank++;
+        if (bse < 0 || k >= A->nLinks) throw Error(CELLS_E_INVALID, "adjoint link table does not match the flags");
+        const AdjLink3Host& Lk = A->hostLinks[(size_t)k];
+        const bool single = Lk.e2 < 0 && Lk.a1 == 1.0;
+        // a single source with coefficient 1 is the plain index; otherwise the sign bit marks the
+        // record's two sources and coefficients
+        sE1[r] = single ? (int)Lk.e1 : (int)((uint32_t)Lk.e1 | 0x80000000u);
+        sE2[r] = Lk.e2 >= 0 ? (int)Lk.e2 : (int)Lk.e1;
+        sA1[r] = Lk.a1;
+        sA2[r] = Lk.e2 >= 0 ? Lk.a2 : 0.0;
+        sTgt[r] = -(k + 1);
+      }
+    }
+  }
+  const size_t nsr = std::max<size_t>(1, 19 * ns);
+  A->sE1 = (int*)dev.alloc(nsr * 4, "adjoint flagged-cell records");
+  A->sE2 = (int*)dev.alloc(nsr * 4, "adjoint flagged-cell records");
+  A->sTgt = (int*)dev.alloc(nsr * 4, "adjoint flagged-cell records");
+  A->sA1 = dev.alloc(nsr * (h->prec == 3 ? 8 : 4), "adjoint flagged-cell records");
+  A->sA2 = dev.alloc(nsr * (h->prec == 3 ? 8 : 4), "adjoint flagged-cell records");
+  if (ns) {
+    dev.h2d(A->sE1, sE1.data(), sE1.size() * 4);
+    dev.h2d(A->sE2, sE2.data(), sE2.size() * 4);
+    dev.h2d(A->sTgt, sTgt.data(), sTgt.size() * 4);
+    dev.sync();
+    if (h->prec == 3) {
+      upload_typed<double>(dev, A->sA1, sA1);
+      upload_typed<double>(dev, A->sA2, sA2);
+    } else {
+      upload_typed<float>(dev, A->sA1, sA1);
+      upload_typed<float>(dev, A->sA2, sA2);
+    }
+  }
   std::vector<long long> e1(L.size()), e2(L.size());
   std::vector<double> a1(L.size()), a2(L.size()), cF(L.size()), q(L.size());
   std::vector<signed char> qk(L.size());
@@ -541,6 +694,135 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
 
 }  // namespace
 
+namespace {
+
+// The launch arguments of the adjoint step kernels for the recorded run (all but f, the adjoint
+// buffers and the step position t, which enqueue_segment sets per step).
+AdjLaunch3 adj_args(Cells3D* h, Adjoint3D* A) {
+  AdjLaunch3 a;
+  std::memset(&a, 0, sizeof(a));
+  a.flags = h->flags;
+  a.xTab = h->xTab;
+  a.linkBase = A->linkBase;
+  a.le1 = A->le1;
+  a.le2 = A->le2;
+  a.la1 = A->la1;
+  a.la2 = A->la2;
+  a.lcF = A->lcF;
+  a.lq = A->lq;
+  a.lqk = A->lqk;
+  a.lamG = A->lamG;
+  a.dqAcc = A->dqAcc;
+  a.blockPart = A->blockPart;
+  a.counter = A->counter;
+  a.N = h->N;
+  a.W = h->W;
+  a.H = h->H;
+  a.D = h->D;
+  a.tileX = A->tileX;
+  a.nCellBlocks = A->nBlocks;
+  a.slowCells = A->slowCells;
+  a.nSlow = A->nSlow;
+  a.sE1 = A->sE1;
+  a.sE2 = A->sE2;
+  a.sTgt = A->sTgt;
+  a.sA1 = A->sA1;
+  a.sA2 = A->sA2;
+  a.nParts = A->nParts;
+  a.nRows = A->nRows;
+  a.rowElem = A->rowElem;
+  a.rowSet = A->rowSet;
+  a.rowStart = A->rowStart;
+  a.entLink = A->entLink;
+  a.entAlpha = A->entAlpha;
+  a.rowPhi = A->rowPhi;
+  a.n0Dev = A->n0Dev;
+  a.uDev = A->uDev;
+  a.wDev = A->wDev;
+  a.dudn = A->dudn;
+  return a;
+}
+
+// Recompute a segment's len states into state set `set` from its checkpoint copy in set[0].
+void enqueue_recompute(Cells3D* h, Adjoint3D* A, int set, int len, int par0, cudaStream_t stream) {
+  for (int t = 0; t + 1 < len; t++) {
+    h->enqueue_step_between(A->seg[set][(size_t)t], A->seg[set][(size_t)t + 1], par0 ^ (t & 1), false, stream);
+    h->dev.launches++;
+  }
+}
+
+// The adjoint steps of a segment whose states are in set `set`, from the last to the first,
+// starting from adjoint buffer c; with `next`, the next (earlier) segment's recompute into the
+// other set runs beside them on side2.
+void enqueue_sweep(Cells3D* h, Adjoint3D* A, AdjLaunch3& a, int set, int len, int c, bool next, int nextLen,
+                   int nextPar0) {
+  cudaStream_t s = h->dev.stream;
+  if (next) {
+    check_cuda(cudaEventRecord(A->fork2, s), "cudaEventRecord");
+    check_cuda(cudaStreamWaitEvent(A->side2, A->fork2, 0), "cudaStreamWaitEvent");
+    enqueue_recompute(h, A, set ^ 1, nextLen, nextPar0, A->side2);
+    check_cuda(cudaEventRecord(A->join2, A->side2), "cudaEventRecord");
+  }
+  for (int t = len - 1; t >= 0; t--) {
+    a.f = A->seg[set][(size_t)t];
+    a.lamNext = A->lam[c];
+    a.lamOut = A->lam[c ^ 1];
+    a.t = t;
+    check_cuda(launch_adjoint_step3(h->prec, a, s, A->side, A->fork, A->join), "adjoint step kernel");
+    h->dev.launches += 3;
+    c ^= 1;
+  }
+  if (next) check_cuda(cudaStreamWaitEvent(s, A->join2, 0), "cudaStreamWaitEvent");
+}
+
+// Full segments replay graphs when K is even (the parity pattern and buffers repeat).
+bool segment_graphs(const Cells3D* h, const Adjoint3D* A) { return h->useGraphs && A->K % 2 == 0; }
+
+void build_segment_graph(Cells3D* h, Adjoint3D* A, int set, int next, int cur) {
+  cudaGraphExec_t& g = A->segGraph[set][next];
+  if (g) cudaGraphExecDestroy(g);
+  g = nullptr;
+  AdjLaunch3 a = adj_args(h, A);
+  const int par0 = A->parity0 & 1;  // the parity at every full segment's start (K even)
+  const int64_t before = h->dev.launches;
+  check_cuda(cudaStreamBeginCapture(h->dev.stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  enqueue_sweep(h, A, a, set, A->K, cur, next != 0, A->K, par0);
+  cudaGraph_t graph = nullptr;
+  check_cuda(cudaStreamEndCapture(h->dev.stream, &graph), "cudaStreamEndCapture");
+  cudaError_t e = cudaGraphInstantiate(&g, graph, 0);
+  cudaGraphDestroy(graph);
+  check_cuda(e, "cudaGraphInstantiate");
+  A->segGraphLaunches[set][next] = h->dev.launches - before;
+  h->dev.launches = before;
+}
+
+// The state set of segment s: the sweep alternates sets, starting with set 0 at the last segment.
+int seg_set(const Adjoint3D* A, int64_t s) {
+  const int64_t nSeg = (A->steps + A->K - 1) / A->K;
+  return (int)((nSeg - 1 - s) & 1);
+}
+
+// The sweep reaches its full segments with adjoint buffer 0, or 1 after an odd-length last segment.
+int full_segment_cur(const Adjoint3D* A) {
+  const int64_t nSeg = (A->steps + A->K - 1) / A->K;
+  const int64_t lenLast = A->steps - (nSeg - 1) * A->K;
+  return (lenLast < A->K && (lenLast & 1)) ? 1 : 0;
+}
+
+void build_segment_graphs(Cells3D* h, Adjoint3D* A) {
+  const int64_t nSeg = (A->steps + A->K - 1) / A->K;
+  const int cur = full_segment_cur(A);
+  for (int64_t s = nSeg - 1; s >= 0; s--) {
+    const int64_t len = std::min<int64_t>(A->K, A->steps - s * A->K);
+    if (len != A->K) continue;
+    const int set = seg_set(A, s), next = s > 0 ? 1 : 0;
+    if (!A->segGraph[set][next]) build_segment_graph(h, A, set, next, cur);
+  }
+  A->segGraphCur = cur;
+}
+
+}  // namespace
+
 // ---------------- C ABI ----------------
 
 #define ADJ_TRY(h) try {
@@ -577,6 +859,7 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
     throw Error(CELLS_E_INVALID, "the objective window must lie within the recorded steps");
   const int64_t nWin = spec->window_end - spec->window_begin + 1;
   if (nWin > HISTORY_LEN) throw Error(CELLS_E_INVALID, "the objective window exceeds the 8192-sample force ring");
+  if (19ll * h->N >= (1ll << 31)) throw Error(CELLS_E_INVALID, "the adjoint supports grids of fewer than 2^31 / 19 cells");
   release_adjoint(h);
   h->adj.reset(new Adjoint3D());
   Adjoint3D* A = h->adj.get();
@@ -591,8 +874,8 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
   cells::Device& dev = h->dev;
   const size_t fBytes = 19ull * h->bpp * (size_t)h->N;
   const int64_t nSeg = (A->steps + A->K - 1) / A->K;
-  const int segBufs = (int)std::min<int64_t>(A->K, A->steps) - 1;
-  const size_t need = (size_t)(nSeg + segBufs + 2) * fBytes + (size_t)h->N * 16;
+  const int segBufs = (int)std::min<int64_t>(A->K, A->steps);
+  const size_t need = (size_t)(nSeg + 2 * segBufs + 2) * fBytes + (size_t)h->N * 16;
   if (need > dev.free_bytes())
     throw AllocError("the adjoint's checkpoints need " + std::to_string(need) + " bytes; the device has " +
                      std::to_string(dev.free_bytes()) + " free");
@@ -601,14 +884,28 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
     A->ck.push_back(dev.alloc(fBytes, "adjoint checkpoint"));
     A->ckState.push_back(dev.alloc(sizeof(DevState3), "adjoint checkpoint"));
   }
-  for (int k = 0; k < segBufs; k++) A->seg.push_back(dev.alloc(fBytes, "adjoint segment"));
+  for (int set = 0; set < 2; set++)
+    for (int k = 0; k < segBufs; k++) A->seg[set].push_back(dev.alloc(fBytes, "adjoint segment"));
   A->endState = dev.alloc(sizeof(DevState3), "adjoint end state");
   A->lam[0] = dev.alloc(fBytes, "adjoint state");
   A->lam[1] = dev.alloc(fBytes, "adjoint state");
-  A->nBlocks = (int)((h->N + kAdjThreads - 1) / kAdjThreads);
-  A->blockPart = (double*)dev.alloc((size_t)A->nBlocks * 8, "adjoint partials");
+  A->tileX = h->W >= 128 ? 128 : (h->W >= 64 ? 64 : 32);
+  const int tileY = kAdjThreads / A->tileX;
+  A->nBlocks = ((h->W + A->tileX - 1) / A->tileX) * ((h->H + tileY - 1) / tileY) * h->D;
+  A->nParts = A->nBlocks + (A->nSlow + kSlowCells - 1) / kSlowCells;
+  A->blockPart = (double*)dev.alloc((size_t)A->nParts * 8, "adjoint partials");
   A->counter = (unsigned*)dev.alloc(64, "adjoint counter");
   A->dudn = (double*)dev.alloc((size_t)A->steps * 8, "adjoint du");
+  A->uDev = (double*)dev.alloc((size_t)A->steps * 8, "adjoint step speeds");
+  A->wDev = (double*)dev.alloc((size_t)A->steps * 8, "adjoint step weights");
+  A->n0Dev = (int*)dev.alloc(64, "adjoint segment index");
+  A->n0Host = (int*)dev.host_pinned((size_t)nSeg * sizeof(int));
+  check_cuda(cudaStreamCreateWithFlags(&A->side, cudaStreamNonBlocking), "cudaStreamCreate");
+  check_cuda(cudaStreamCreateWithFlags(&A->side2, cudaStreamNonBlocking), "cudaStreamCreate");
+  check_cuda(cudaEventCreateWithFlags(&A->fork2, cudaEventDisableTiming), "cudaEventCreate");
+  check_cuda(cudaEventCreateWithFlags(&A->join2, cudaEventDisableTiming), "cudaEventCreate");
+  check_cuda(cudaEventCreateWithFlags(&A->fork, cudaEventDisableTiming), "cudaEventCreate");
+  check_cuda(cudaEventCreateWithFlags(&A->join, cudaEventDisableTiming), "cudaEventCreate");
   // the recorded run: a checkpoint at the start of every segment, force samples in the window
   const uint64_t written0 = h->forceSamplesRead + h->forceSteps.size();
   A->uStep.resize((size_t)A->steps);
@@ -649,8 +946,18 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
   double sum = 0.0;
   for (const double4& v : hist) sum += A->component == 0 ? v.x : (A->component == 1 ? v.y : v.z);
   A->objective = A->scale * sum / (double)nWin;
+  std::vector<double> wStep((size_t)A->steps, 0.0);
+  for (int64_t n = 0; n < A->steps; n++) {
+    const int64_t label = s0 + n + 1;
+    if (label >= A->w0 && label <= A->w1) wStep[(size_t)n] = A->scale / (double)nWin;
+  }
+  dev.h2d(A->uDev, A->uStep.data(), (size_t)A->steps * 8);
+  dev.h2d(A->wDev, wStep.data(), (size_t)A->steps * 8);
+  dev.sync();
   A->endStep = h->step;
   A->argGen = h->argGen;
+  // the backward sweep's segment graphs, built now (record time) rather than inside the sweep
+  if (segment_graphs(h, A)) build_segment_graphs(h, A);
   if (objective) *objective = A->objective;
   ADJ_CATCH(h)
 }
@@ -676,61 +983,40 @@ int cells3d_adjoint_backward(Cells3D* h, const void* terminal_adjoint, double* d
     dev.h2d(A->lam[0], terminal_adjoint, fBytes);
     dev.sync();
   }
-  const int64_t nWin = A->w1 - A->w0 + 1;
   const int64_t nSeg = (A->steps + A->K - 1) / A->K;
-  AdjLaunch3 a;
-  std::memset(&a, 0, sizeof(a));
-  a.flags = h->flags;
-  a.xTab = h->xTab;
-  a.linkBase = A->linkBase;
-  a.le1 = A->le1;
-  a.le2 = A->le2;
-  a.la1 = A->la1;
-  a.la2 = A->la2;
-  a.lcF = A->lcF;
-  a.lq = A->lq;
-  a.lqk = A->lqk;
-  a.lamG = A->lamG;
-  a.dqAcc = A->dqAcc;
-  a.blockPart = A->blockPart;
-  a.counter = A->counter;
-  a.N = N;
-  a.W = h->W;
-  a.H = h->H;
-  a.D = h->D;
-  a.nRows = A->nRows;
-  a.rowElem = A->rowElem;
-  a.rowSet = A->rowSet;
-  a.rowStart = A->rowStart;
-  a.entLink = A->entLink;
-  a.entAlpha = A->entAlpha;
-  a.rowPhi = A->rowPhi;
-  for (int64_t sgi = nSeg - 1; sgi >= 0; sgi--) {
-    const int64_t n0 = sgi * A->K;
-    const int len = (int)std::min<int64_t>(A->K, A->steps - n0);
-    // recompute the segment's states from its checkpoint (no force sampling)
-    check_cuda(cudaMemcpyAsync(h->st, A->ckState[(size_t)sgi], sizeof(DevState3), cudaMemcpyDeviceToDevice,
+  AdjLaunch3 a = adj_args(h, A);
+  const bool graphs = segment_graphs(h, A);
+  if (graphs && A->segGraphCur != full_segment_cur(A)) build_segment_graphs(h, A);
+  // restore a segment's device state and first state (its checkpoint) into its state set
+  auto restore = [&](int64_t s) {
+    check_cuda(cudaMemcpyAsync(h->st, A->ckState[(size_t)s], sizeof(DevState3), cudaMemcpyDeviceToDevice,
                                dev.stream),
                "checkpoint restore");
-    auto state = [&](int t) -> void* { return t == 0 ? A->ck[(size_t)sgi] : A->seg[(size_t)(t - 1)]; };
-    const int par0 = (int)((A->parity0 + n0) & 1);
-    for (int t = 0; t + 1 < len; t++) {
-      h->enqueue_step_between(state(t), state(t + 1), par0 ^ (t & 1), false);
-      dev.launches++;
+    check_cuda(cudaMemcpyAsync(A->seg[seg_set(A, s)][0], A->ck[(size_t)s], fBytes, cudaMemcpyDeviceToDevice,
+                               dev.stream),
+               "checkpoint restore");
+  };
+  auto seg_len = [&](int64_t s) { return (int)std::min<int64_t>(A->K, A->steps - s * A->K); };
+  auto seg_par0 = [&](int64_t s) { return (int)((A->parity0 + s * A->K) & 1); };
+  // the last segment's states first; every other segment's recompute runs beside the sweep of the
+  // segment after it
+  restore(nSeg - 1);
+  enqueue_recompute(h, A, seg_set(A, nSeg - 1), seg_len(nSeg - 1), seg_par0(nSeg - 1), dev.stream);
+  for (int64_t sgi = nSeg - 1; sgi >= 0; sgi--) {
+    const int len = seg_len(sgi);
+    const int set = seg_set(A, sgi);
+    const bool next = sgi > 0;
+    A->n0Host[sgi] = (int)(sgi * A->K);
+    check_cuda(cudaMemcpyAsync(A->n0Dev, A->n0Host + sgi, sizeof(int), cudaMemcpyHostToDevice, dev.stream),
+               "segment index copy");
+    if (next) restore(sgi - 1);
+    if (graphs && len == A->K && cur == A->segGraphCur) {
+      check_cuda(cudaGraphLaunch(A->segGraph[set][next ? 1 : 0], dev.stream), "cudaGraphLaunch");
+      dev.launches += A->segGraphLaunches[set][next ? 1 : 0];
+    } else {
+      enqueue_sweep(h, A, a, set, len, cur, next, next ? seg_len(sgi - 1) : 0, next ? seg_par0(sgi - 1) : 0);
     }
-    for (int t = len - 1; t >= 0; t--) {
-      const int64_t n = n0 + t;
-      const int64_t label = A->s0 + n + 1;
-      a.f = state(t);
-      a.lamNext = A->lam[cur];
-      a.lamOut = A->lam[cur ^ 1];
-      a.u = A->uStep[(size_t)n];
-      a.w = (label >= A->w0 && label <= A->w1) ? A->scale / (double)nWin : 0.0;
-      a.dudOut = A->dudn + n;
-      check_cuda(launch_adjoint_step3(h->prec, a, dev.stream), "adjoint step kernel");
-      dev.launches += 2;
-      cur ^= 1;
-    }
+    if (len & 1) cur ^= 1;
   }
   check_cuda(cudaMemcpyAsync(h->st, A->endState, sizeof(DevState3), cudaMemcpyDeviceToDevice, dev.stream),
              "end state restore");

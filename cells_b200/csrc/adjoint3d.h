@@ -47,7 +47,7 @@ struct Adjoint3D {
   std::vector<void*> ck;
   std::vector<void*> ckState;
   void* endState = nullptr;  // device state after the run (restored after the backward sweep)
-  std::vector<void*> seg;    // K recomputed states of the current segment
+  std::vector<void*> seg[2];  // two sets of K recomputed states: the segment being swept and the next
 
   // link tables (device)
   int nLinks = 0;
@@ -77,7 +77,28 @@ struct Adjoint3D {
   double* blockPart = nullptr;
   unsigned* counter = nullptr;
   double* dudn = nullptr;            // dJ/du_n per recorded step
-  int nBlocks = 0;
+  int nBlocks = 0;  // blocks of the cell kernel
+  int tileX = 128;
+  double* uDev = nullptr;    // inlet speed of each recorded step (device)
+  double* wDev = nullptr;    // objective weight of each recorded step (device)
+  int* n0Dev = nullptr;      // first step of the segment being swept (device)
+  int* n0Host = nullptr;     // pinned, one slot per segment (the source of each n0Dev copy)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaStream_t side2 = nullptr;          // the next segment's recompute, beside the sweep
+  cudaEvent_t fork2 = nullptr, join2 = nullptr;
+  // full segments replay captured graphs: [state set of the swept segment][with the next recompute]
+  cudaGraphExec_t segGraph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int64_t segGraphLaunches[2][2] = {{0, 0}, {0, 0}};
+  int segGraphCur = -1;                 // the adjoint buffer the graphs start from
+  int* slowCells = nullptr;  // flagged fluid cells (device), in index order
+  int nSlow = 0;
+  int* sE1 = nullptr;        // [19][nSlow] pull records of the flagged cells
+  int* sE2 = nullptr;
+  int* sTgt = nullptr;
+  void* sA1 = nullptr;       // R
+  void* sA2 = nullptr;       // R
+  int nParts = 0;            // entries of blockPart
 };
 
 namespace cells {
@@ -100,11 +121,24 @@ struct AdjLaunch3 {
   double* dqAcc;
   double* blockPart;
   unsigned* counter;
-  double* dudOut;        // &dudn[n]
+  const int* n0Dev;      // first recorded step of the current segment (device)
+  int t;                 // this step's position in the segment: step n = *n0Dev + t
+  const double* uDev;    // inlet speed of each recorded step
+  const double* wDev;    // objective weight of each recorded step's force
+  double* dudn;          // dJ/du_n of each recorded step
   long long N;
   int W, H, D;
-  double u;              // inlet speed of the step
-  double w;              // objective weight of the step's force
+  int tileX;             // cell kernel block: tileX x (kAdjThreads / tileX) cells of x-rows
+  int nCellBlocks;       // blocks of the cell kernel
+  const int* slowCells;  // the flagged fluid cells, in index order
+  int nSlow;
+  const int* sE1;        // [19][nSlow]: the source of a one-source pull (coefficient 1), or the first
+                         // of two sources with the sign bit set (then sE2, sA1, sA2 apply)
+  const int* sE2;
+  const int* sTgt;       // [19][nSlow]: element of a plain pull's adjoint, or -(link + 1)
+  const void* sA1;       // R: coefficients (a2 = 0 for one source)
+  const void* sA2;
+  int nParts;            // blockPart entries: nCellBlocks + blocks of the flagged-cell kernel
   // transposed map
   int nRows;
   const long long* rowElem;
@@ -116,7 +150,10 @@ struct AdjLaunch3 {
 };
 
 constexpr int kAdjThreads = 128;
-// one adjoint step: the per-cell kernel, then the boundary-element kernel (precision 0 or 3)
-cudaError_t launch_adjoint_step3(int precision, const AdjLaunch3& a, cudaStream_t s);
+// One adjoint step (precision 0 or 3): the interior-cell kernel on `s` and the flagged-cell kernel
+// on `side` run concurrently (they write disjoint elements), then the boundary-element kernel on
+// `s`. fork and join are events used to order the two streams.
+cudaError_t launch_adjoint_step3(int precision, const AdjLaunch3& a, cudaStream_t s, cudaStream_t side,
+                                 cudaEvent_t fork, cudaEvent_t join);
 
 }  // namespace cells

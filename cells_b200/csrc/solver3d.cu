@@ -169,8 +169,8 @@ int Cells3D::enqueue_step(int par, bool sample, cudaStream_t main) {
   return 1;
 }
 
-void Cells3D::enqueue_step_between(const void* src, void* dst, int par, bool sample) {
-  cudaStream_t main = dev.stream;
+void Cells3D::enqueue_step_between(const void* src, void* dst, int par, bool sample, cudaStream_t stream) {
+  cudaStream_t main = stream ? stream : dev.stream;
   StepLaunch3 a;
   a.src = src;
   a.dst = dst;
@@ -722,6 +722,75 @@ int cells3d_write_populations(Cells3D* h, const void* in, size_t bytes) {
   if (bytes != need) throw Error(CELLS_E_INVALID, "write_populations needs " + std::to_string(need) + " bytes");
   h->dev.h2d(h->f[h->parity], in, need);
   h->dev.sync();
+  CELLS_CATCH(h)
+}
+
+// Snapshot layout: this header, then 19 N populations of the storage type.
+struct StateHeader3 {
+  uint64_t magic;  // "CELLS3D1"
+  int32_t W, H, D, precision;
+  int64_t step;
+  int32_t parity, rampKind;
+  double uIn, rampTarget;
+  int64_t rampSteps, rampEvery;
+};
+static constexpr uint64_t kStateMagic3 = 0x3144334c4c4543ull;
+
+int cells3d_state_size(Cells3D* h, size_t* bytes) {
+  if (!h || !bytes) return CELLS_E_INVALID;
+  *bytes = sizeof(StateHeader3) + 19ull * h->bpp * (size_t)h->N;
+  return CELLS_OK;
+}
+
+int cells3d_save_state(Cells3D* h, void* out, size_t bytes) {
+  if (!h || !out) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  const size_t pop = 19ull * h->bpp * (size_t)h->N;
+  if (bytes != sizeof(StateHeader3) + pop) throw Error(CELLS_E_INVALID, "save_state needs state_size bytes");
+  StateHeader3 s{};
+  s.magic = kStateMagic3;
+  s.W = h->W;
+  s.H = h->H;
+  s.D = h->D;
+  s.precision = h->prec;
+  s.step = h->step;
+  s.parity = h->parity;
+  s.rampKind = h->rampKind;
+  s.uIn = h->uIn;
+  s.rampTarget = h->rampTarget;
+  s.rampSteps = h->rampSteps;
+  s.rampEvery = h->rampEvery;
+  std::memcpy(out, &s, sizeof(s));
+  h->dev.d2h((char*)out + sizeof(s), h->f[h->parity], pop);
+  h->dev.sync();
+  CELLS_CATCH(h)
+}
+
+int cells3d_load_state(Cells3D* h, const void* in, size_t bytes) {
+  if (!h || !in) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  const size_t pop = 19ull * h->bpp * (size_t)h->N;
+  if (bytes != sizeof(StateHeader3) + pop) throw Error(CELLS_E_INVALID, "load_state needs state_size bytes");
+  StateHeader3 s;
+  std::memcpy(&s, in, sizeof(s));
+  if (s.magic != kStateMagic3) throw Error(CELLS_E_INVALID, "not a Solver3D state snapshot");
+  if (s.W != h->W || s.H != h->H || s.D != h->D || s.precision != h->prec)
+    throw Error(CELLS_E_INVALID, "the snapshot's grid or precision differs from this solver's");
+  h->step = s.step;
+  h->parity = s.parity & 1;
+  h->uIn = s.uIn;
+  h->cfg.u_in = s.uIn;
+  h->rampKind = s.rampKind;
+  h->rampTarget = s.rampTarget;
+  h->rampSteps = s.rampSteps > 0 ? s.rampSteps : 1;
+  h->rampEvery = s.rampEvery > 0 ? s.rampEvery : 1;
+  h->argGen++;
+  h->dev.h2d(h->f[h->parity], (const char*)in + sizeof(s), pop);
+  h->dev.sync();
+  h->write_state(1 | 2 | 4);
+  h->forceSamplesRead = 0;
+  h->forceSteps.clear();
+  h->forceGeneration++;
   CELLS_CATCH(h)
 }
 

@@ -104,8 +104,9 @@ struct Cells3D : cells::HandleBase {
   void rebuild_flags();
   void build_body_list(const std::vector<uint8_t>& rows);
   int enqueue_step(int par, bool sample, cudaStream_t main);
-  // one step from src to dst (any buffers of 19 N populations), parity par of the device state
-  void enqueue_step_between(const void* src, void* dst, int par, bool sample);
+  // one step from src to dst (any buffers of 19 N populations), parity par of the device state, on
+  // `stream` (nullptr: the handle's stream)
+  void enqueue_step_between(const void* src, void* dst, int par, bool sample, cudaStream_t stream = nullptr);
   int graph_period() const;
   void build_graph(int phase);
   void launch_steps(int64_t n);

@@ -207,6 +207,20 @@ class Solver3D:
         check(lib().cells3d_read_flags(self._h, out.ctypes.data, out.size), self._h)
         return out
 
+    # ------------------------------------------------------------------ state save / restore
+    def saveState(self) -> bytes:
+        """Snapshot of the populations, step, parity, inlet speed and ramp (not the SDF or parameters)."""
+        n = C.c_size_t()
+        check(lib().cells3d_state_size(self._h, C.byref(n)), self._h)
+        buf = (C.c_uint8 * n.value)()
+        check(lib().cells3d_save_state(self._h, buf, n.value), self._h)
+        return bytes(buf)
+
+    def loadState(self, state: bytes) -> None:
+        """Restores a saveState snapshot into a solver with the same grid, precision, config and SDF."""
+        b = (C.c_uint8 * len(state)).from_buffer_copy(state)
+        check(lib().cells3d_load_state(self._h, b, len(state)), self._h)
+
     # ------------------------------------------------------------------ discrete adjoint
     def adjointForward(self, steps: int, windowBegin: int, windowEnd: int, checkpointEvery: int = 100,
                        component: int = 0, scale: float = 1.0) -> float:

@@ -219,6 +219,15 @@ int cells3d_adjoint_backward(Cells3D* h, const void* terminal_adjoint, double* d
 /* Frees the recorded run's checkpoints and tables. */
 int cells3d_adjoint_release(Cells3D* h);
 
+/* ---------------- state save / restore (no counterpart in the reference) ----------------
+ * A snapshot of the simulation state for resuming long runs: the latest populations, the step
+ * count, the parity, the inlet speed and the device-side ramp. The geometry (SDF) and the
+ * parameters are not included: restore into a handle created with the same config and SDF.
+ * Loading resets the force ring (like init_field). */
+int cells3d_state_size(Cells3D* h, size_t* bytes);
+int cells3d_save_state(Cells3D* h, void* out, size_t bytes);
+int cells3d_load_state(Cells3D* h, const void* in, size_t bytes);
+
 /* ---------------- timing (CUDA events on the handle's stream) ---------------- */
 int cells3d_timer_start(Cells3D* h);
 int cells3d_timer_stop(Cells3D* h, float* ms);

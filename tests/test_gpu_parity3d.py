@@ -86,6 +86,21 @@ def test_sphere_fast_fp32_within_tolerance():
     s.destroy()
 
 
+@pytest.mark.parametrize("precision,tol", [("fp16", 1e-4), ("bf16", 1e-3)])
+def test_sphere_fast_16bit_within_storage_rounding(precision, tol):
+    """Fast arithmetic with 16-bit storage (the x-pair path with packed dual-FP32 collisions) stays
+    within a few storage ulps of the exact oracle after 30 steps: FP16 x 2^15 has an ulp of about
+    3e-5 at |f - w| = 0.05, BF16 about 2.4e-4."""
+    W, H, D = 32, 16, 12
+    s, o = pair(W, H, D, precision, False, sphere_sdf(W, H, D, 10, 8, 6, 3))
+    for n in (1, 29):
+        s.encodeSteps(n)
+        o.encodeSteps(n)
+        assert_same(s, o, False, tol)
+    assert_forces(s.readForces(), o.readForces(), 2e-2)
+    s.destroy()
+
+
 def test_smagorinsky_fixed_lambda_cylinder_touching_slip_faces():
     """A spanwise cylinder meets both z faces: the slip-face bounce-back with its force branch."""
     W, H, D = 20, 12, 10
@@ -215,3 +230,28 @@ def test_graph_replay_matches_oracle(every):
     assert_forces(s.readForces(), o.readForces(), 1e-9)
     assert s.launchCount() >= 596  # one step kernel per step, whether replayed from a graph or not
     s.destroy()
+
+
+def test_state_snapshot_resumes_bit_for_bit():
+    """saveState after 137 steps, loadState into a fresh solver with the same SDF: the next 150 steps
+    (ramp still running) give the same populations as the uninterrupted run."""
+    W, H, D = 24, 16, 12
+    sdf = sphere_sdf(W, H, D, 8, 8, 6, 3)
+    cfg = dict(BASE, uIn=0.0)
+    s = Solver3D.create(W, H, D, precision="fp32", exactArithmetic=True, **cfg)
+    s.setSdf(sdf)
+    s.initField(perturbed_rest3(W, H, D, 1e-4))
+    s.setInletRamp("smoothstep", 0.08, 200, 1)
+    s.encodeSteps(137)
+    snap = s.saveState()
+    s.encodeSteps(150)
+    t = Solver3D.create(W, H, D, precision="fp32", exactArithmetic=True, **cfg)
+    t.setSdf(sdf)
+    t.loadState(snap)
+    t.encodeSteps(150)
+    a, b = s.readPopulations(), t.readPopulations()
+    solid = np.tile((s.readFlags() & (1 << 19)) != 0, 19)
+    assert np.array_equal(a.view(np.uint32)[~solid], b.view(np.uint32)[~solid])
+    assert t.step == s.step == 287
+    s.destroy()
+    t.destroy()

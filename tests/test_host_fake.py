@@ -149,3 +149,25 @@ def test_force_every_zero_disables_sampling():
     s.encodeSteps(100)
     assert s.readForces() == []
     s.destroy()
+
+
+def test_state_snapshot_round_trip_and_checks():
+    s = fake(forceEvery=2)
+    s.setInletRamp("linear", 0.1, 300, 1)
+    s.encodeSteps(7)
+    snap = s.saveState()
+    t = fake(forceEvery=2)
+    t.loadState(snap)
+    assert t.step == 7
+    assert t.readParams() == s.readParams()
+    assert t.readForces() == []
+    with pytest.raises(_lib.CellsError):
+        t.loadState(snap[:-1])
+    with pytest.raises(_lib.CellsError):
+        fake(width=9).loadState(snap)
+    bad = bytearray(snap)
+    bad[0] ^= 1
+    with pytest.raises(_lib.CellsError):
+        t.loadState(bytes(bad))
+    s.destroy()
+    t.destroy()

@@ -114,21 +114,46 @@ __device__ __forceinline__ void collide3(const StepArgs3<C>& a, const typename C
                                          typename C::R (&o)[Q3]) {
   using R = typename C::R;
   constexpr R IS = R(1) / R(C::SCALE);
-  // moments, in the generated WGSL's left-to-right order
-  R dsum = f[0];
+  // 16-bit storage is issue-bound rather than bandwidth-bound, so its fast arithmetic uses the
+  // leanest form: the pair sums s_p = f_p + f_p+1 and differences d_p = f_p - f_p+1 (p odd) feed both
+  // the moments and the TRT update. Wider storage keeps the form with fewer live registers.
+  constexpr bool kLean = !kExact && sizeof(typename C::S) == 2;
+  R sp[Q3], dp[Q3];
+  R drho, rho, ux, uy, uz, invRho;
+  if constexpr (!kLean) {
+    // moments, in the generated WGSL's left-to-right order
+    R dsum = f[0];
 #pragma unroll
-  for (int i = 1; i < Q3; i++) dsum = dsum + f[i];
-  const R drho = dsum * IS;
-  const R rho = R(1) + drho;
-  // fast arithmetic: the hardware reciprocal (branch-free, within 2 ulp) instead of IEEE division
-  R invRho;
-  if constexpr (!kExact && sizeof(R) == 4)
-    invRho = __fdividef(R(1), rho);
-  else
-    invRho = R(1) / rho;
-  const R ux = ((f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[13] - f[14] + f[15] - f[16]) * IS) * invRho;
-  const R uy = ((f[3] - f[4] + f[7] - f[8] + f[11] - f[12] - f[13] + f[14] + f[17] - f[18]) * IS) * invRho;
-  const R uz = ((f[5] - f[6] + f[9] - f[10] + f[11] - f[12] - f[15] + f[16] - f[17] + f[18]) * IS) * invRho;
+    for (int i = 1; i < Q3; i++) dsum = dsum + f[i];
+    drho = dsum * IS;
+    rho = R(1) + drho;
+    // fast arithmetic: the hardware reciprocal (branch-free, within 2 ulp) instead of IEEE division
+    if constexpr (!kExact && sizeof(R) == 4)
+      invRho = __fdividef(R(1), rho);
+    else
+      invRho = R(1) / rho;
+    ux = ((f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[13] - f[14] + f[15] - f[16]) * IS) * invRho;
+    uy = ((f[3] - f[4] + f[7] - f[8] + f[11] - f[12] - f[13] + f[14] + f[17] - f[18]) * IS) * invRho;
+    uz = ((f[5] - f[6] + f[9] - f[10] + f[11] - f[12] - f[15] + f[16] - f[17] + f[18]) * IS) * invRho;
+  } else {
+#pragma unroll
+    for (int p = 1; p < Q3; p += 2) {
+      sp[p] = f[p] + f[p + 1];
+      dp[p] = f[p] - f[p + 1];
+    }
+    drho = (f[0] + ((sp[1] + sp[3]) + (sp[5] + sp[7])) + ((sp[9] + sp[11]) + (sp[13] + (sp[15] + sp[17])))) * IS;
+    rho = R(1) + drho;
+    // the hardware reciprocal (branch-free, within 2 ulp) instead of IEEE division, with 1/SCALE folded in
+    R invRhoS;
+    if constexpr (sizeof(R) == 4)
+      invRhoS = __fdividef(IS, rho);
+    else
+      invRhoS = IS / rho;
+    invRho = invRhoS * R(C::SCALE);  // exact: SCALE is a power of two
+    ux = (((dp[1] + dp[7]) + (dp[9] + dp[13])) + dp[15]) * invRhoS;
+    uy = (((dp[3] + dp[7]) + (dp[11] - dp[13])) + dp[17]) * invRhoS;
+    uz = (((dp[5] + dp[9]) + (dp[11] - dp[15])) - dp[17]) * invRhoS;
+  }
   const R usq = R(1.5) * (ux * ux + uy * uy + uz * uz);
   if (outlet) {
     // pressure outlet: equilibrium at rho = 1 with the node's own velocity; fast arithmetic uses
@@ -212,6 +237,47 @@ __device__ __forceinline__ void collide3(const StepArgs3<C>& a, const typename C
       o[p + 1] = f[p + 1] - sym + asym + sS - sA;
     }
   } else {
+   if constexpr (kLean) {
+    // e_p = rho cu^2 / 2 + K0 with K0 = drho - rho usq, so with cP = omega+ w and cM = omega- w rho:
+    //   A = cP e - omega+/2 s_p = (cP rho / 2) cu cu + (cP K0 - omega+/2 s_p)
+    //   B = cM cu - omega-/2 d_p
+    const R K0 = drho - rho * usq;
+    const R nhP = R(-0.5) * omP, nhM = R(-0.5) * omM;
+    const R u3[3] = {R(3) * ux, R(3) * uy, R(3) * uz};
+    const R cP0 = omP * ws3<C>(1), cP1 = omP * ws3<C>(7);
+    const R cPr[2] = {cP0 * (R(0.5) * rho), cP1 * (R(0.5) * rho)};
+    const R cK[2] = {cP0 * K0, cP1 * K0};
+    const R cM[2] = {omM * ws3<C>(1) * rho, omM * ws3<C>(7) * rho};
+    R v0 = f[0] - omP * (f[0] - ws3<C>(0) * K0);
+    if (absorb) v0 += sigma * ws3<C>(0) * -dq;
+    o[0] = v0;
+#pragma unroll
+    for (int p = 1; p < Q3; p += 2) {
+      const int k = p <= 5 ? 0 : 1;
+      R cu;
+      switch (p) {  // 3 (c_p . u) from the precomputed 3u
+        case 1: cu = u3[0]; break;
+        case 3: cu = u3[1]; break;
+        case 5: cu = u3[2]; break;
+        case 7: cu = u3[0] + u3[1]; break;
+        case 9: cu = u3[0] + u3[2]; break;
+        case 11: cu = u3[1] + u3[2]; break;
+        case 13: cu = u3[0] - u3[1]; break;
+        case 15: cu = u3[0] - u3[2]; break;
+        default: cu = u3[1] - u3[2]; break;
+      }
+      R A = (cPr[k] * cu) * cu + (cK[k] + nhP * sp[p]);
+      R B = cM[k] * cu + nhM * dp[p];
+      if (absorb) {
+        const R cut = R(3) * R(cx3(p)) * ut;
+        const R sw = sigma * ws3<C>(p);
+        A += sw * (R(0.5) * rho * (cut * cut - cu * cu) - dq);
+        B += sw * rho * (cut - cu);
+      }
+      o[p] = f[p] + A + B;
+      o[p + 1] = f[p + 1] + A - B;
+    }
+   } else {
     const R hP = R(0.5) * omP, hM = R(0.5) * omM;
     const R u3[3] = {R(3) * ux, R(3) * uy, R(3) * uz};
     const R cP[2] = {omP * ws3<C>(1), omP * ws3<C>(7)};
@@ -246,8 +312,10 @@ __device__ __forceinline__ void collide3(const StepArgs3<C>& a, const typename C
       o[p] = f[p] + A + B;
       o[p + 1] = f[p + 1] + A - B;
     }
+   }
   }
 }
+
 
 template <class C, bool SMAG>
 __device__ __forceinline__ void collide_store(const StepArgs3<C>& a, const typename C::R (&f)[Q3], int x, int idx,
@@ -588,7 +656,8 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
   }
   if (act0 && act1) {
 #pragma unroll
-    for (int i = 0; i < Q3; i++) *reinterpret_cast<uint32_t*>(a.out[i] + idx) = C::pack2(o0[i], o1[i]);
+    for (int i = 0; i < Q3; i++)
+      *reinterpret_cast<uint32_t*>(a.out[i] + idx) = kExact ? C::pack2(o0[i], o1[i]) : C::pack2_fast(o0[i], o1[i]);
   } else if (act0) {
 #pragma unroll
     for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(o0[i]);

@@ -88,9 +88,9 @@ def test_sphere_fast_fp32_within_tolerance():
 
 @pytest.mark.parametrize("precision,tol", [("fp16", 1e-4), ("bf16", 1e-3)])
 def test_sphere_fast_16bit_within_storage_rounding(precision, tol):
-    """Fast arithmetic with 16-bit storage (the x-pair path with packed dual-FP32 collisions) stays
-    within a few storage ulps of the exact oracle after 30 steps: FP16 x 2^15 has an ulp of about
-    3e-5 at |f - w| = 0.05, BF16 about 2.4e-4."""
+    """Fast arithmetic with 16-bit storage (the x-pair path with the lean TRT form and saturating
+    stores) stays within a few storage ulps of the exact oracle after 30 steps: FP16 x 2^15 has an
+    ulp of about 3e-5 at |f - w| = 0.05, BF16 about 2.4e-4."""
     W, H, D = 32, 16, 12
     s, o = pair(W, H, D, precision, False, sphere_sdf(W, H, D, 10, 8, 6, 3))
     for n in (1, 29):

@@ -68,6 +68,11 @@ struct Cells3D : cells::HandleBase {
   // the discrete adjoint's recorded forward run (checkpoints, link tables), when one exists
   std::unique_ptr<Adjoint3D> adj;
 
+  // device scratch of the macro-field products (fields3d.cu), grown on demand
+  void* scratch = nullptr;
+  size_t scratchBytes = 0;
+  void* scratch_buffer(size_t bytes);
+
   double lambda_value() const {
     if (std::isnan(cfg.lambda)) return std::fmin(3.0 / 16.0, 50.0 * (cfg.tau - 0.5) * (cfg.tau - 0.5));
     return cfg.lambda;

@@ -207,6 +207,38 @@ class Solver3D:
         check(lib().cells3d_read_flags(self._h, out.ctypes.data, out.size), self._h)
         return out
 
+    # ------------------------------------------------------------------ macro-field products
+    FIELD_MODES = {"speed": 0, "vorticity": 1}
+    _IN_PLANE = {0: (1, 2), 1: (0, 2), 2: (0, 1)}
+
+    def sampleSlice(self, axis: int, pos: float, mode: str = "speed", uRef: float = 0.1,
+                    size: Optional[tuple] = None) -> np.ndarray:
+        """The slice view of src/shaders/render3d.ts:159-177 without a graphics pipeline: the field
+        (speed / (1.6 uRef) or |curl u| / (0.3 uRef)) at the pixel centres of an (nv, nu) grid over
+        the axis-aligned quad at pos * (dim - 1) on `axis`; NaN on solid nodes. The default size is
+        the in-plane grid, one pixel per cell centre. Reads the macro field of the last run or
+        updateMacro."""
+        dims = (self.W, self.H, self.D)
+        a, b = self._IN_PLANE[axis] if axis in self._IN_PLANE else (0, 0)
+        nu, nv = size if size is not None else (dims[a], dims[b])
+        out = np.empty((nv, nu), dtype=np.float32)
+        check(lib().cells3d_sample_slice(self._h, axis, float(pos), self.FIELD_MODES.get(mode, -1), float(uRef),
+                                         nu, nv, out.ctypes.data), self._h)
+        return out
+
+    def advectTracers(self, seeds: np.ndarray, particles: np.ndarray, steps: float, uRef: float = 0.1) -> None:
+        """One frame of tracer advection (src/shaders/render3d.ts:196-230) over `steps` lattice steps:
+        particles (count, 8) float32 = (x, y, z, 0, ux, uy, uz, 0), updated in place; seeds
+        (count, 4) float32, where a tracer restarts when it leaves the box or enters a solid."""
+        seeds = np.ascontiguousarray(seeds, dtype=np.float32)
+        if particles.dtype != np.float32 or not particles.flags.c_contiguous:
+            raise ValueError("particles must be a C-contiguous float32 array")
+        count = particles.size // 8
+        if particles.size != 8 * count or seeds.size != 4 * count:
+            raise ValueError("particles must hold 8 and seeds 4 floats per tracer")
+        check(lib().cells3d_advect_tracers(self._h, seeds.ctypes.data, particles.ctypes.data, count, float(steps),
+                                           float(uRef)), self._h)
+
     # ------------------------------------------------------------------ state save / restore
     def saveState(self) -> bytes:
         """Snapshot of the populations, step, parity, inlet speed and ramp (not the SDF or parameters)."""

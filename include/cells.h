@@ -174,6 +174,21 @@ int cells3d_read_populations(Cells3D* h, void* out, size_t bytes);
 int cells3d_write_populations(Cells3D* h, const void* in, size_t bytes);
 int cells3d_read_flags(Cells3D* h, uint32_t* out, size_t n);
 
+/* ---------------- macro-field products (src/shaders/render3d.ts:33-65, 159-230) ----------------
+ * Both read the macro buffer as of the last cells3d_update_macro or cells3d_run, as the
+ * reference's slice and tracer passes read solver.macro, and wait for the result. */
+#define CELLS_FIELD_SPEED 0     /* |u| / (1.6 u_ref), the slice's speed mode */
+#define CELLS_FIELD_VORTICITY 1 /* |curl u| / (0.3 u_ref), curl from trilinear velocity at +-1 cell */
+/* The slice quad of sliceShader (render3d.ts:159-177): axis 0/1/2 = x/y/z at pos * (dim - 1),
+ * pos in [0, 1]; the two other axes span [-0.5, dim - 0.5] in order (y, z), (x, z) or (x, y) and are
+ * sampled at the centres of nu x nv pixels: out[j * nu + i]. Solid nodes (nearest node, ties to
+ * even) give NaN. With nu and nv equal to the in-plane dimensions the pixels are the cell centres. */
+int cells3d_sample_slice(Cells3D* h, int axis, double pos, int mode, double u_ref, int nu, int nv, float* out);
+/* advectShader (render3d.ts:196-230): one frame of `steps` lattice steps for `count` tracers.
+ * particles: count x 8 floats (x, y, z, 0, ux, uy, uz, 0), updated in place; seeds: count x 4
+ * floats (x, y, z, 0), where a tracer restarts when it leaves the box or enters a solid. */
+int cells3d_advect_tracers(Cells3D* h, const float* seeds, float* particles, int count, double steps, double u_ref);
+
 /* Allocation-free mass reduction. It has no counterpart in the reference. It is for callers that
  * cannot allocate device memory when they need the result: code inside a CUDA stream capture,
  * hosts that fix their device memory at start-up, real-time loops that must not risk the failure

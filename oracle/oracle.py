@@ -65,6 +65,12 @@ def lib():
         L.oracle_num_threads.restype = C.c_int
         for fn in ("oracle3d_step", "oracle3d_flags", "oracle3d_init", "oracle3d_macro", "oracle3d_mass"):
             getattr(L, fn).restype = C.c_int
+        I = C.c_int
+        F = C.c_float
+        L.oracle3d_sample_slice.argtypes = [P, I, I, I, I, F, I, F, I, I, P]
+        L.oracle3d_sample_slice.restype = I
+        L.oracle3d_advect.argtypes = [P, I, I, I, P, P, I, F, F]
+        L.oracle3d_advect.restype = I
         HP2 = C.POINTER(HostParams2)
         L.oracle2d_step.argtypes = [C.c_int, HP2, P, P, P, P, P]
         L.oracle2d_run.argtypes = [C.c_int, HP2, P, P, C.c_int, C.c_longlong, P, P]
@@ -312,6 +318,25 @@ class OracleSolver2D:
         v = C.c_double()
         lib().oracle2d_mass(self.prec, C.byref(p), _ptr(self.f[self.parity]), _ptr(self.flags), C.byref(v))
         return v.value
+
+
+def sample_slice(mac, W, H, D, axis, pos, mode, uRef, nu, nv):
+    """The oracle's slice of a macro field (4N float32): (nv, nu) float32, NaN on solid nodes."""
+    mac = np.ascontiguousarray(mac, dtype=np.float32)
+    out = np.empty((nv, nu), dtype=np.float32)
+    rc = lib().oracle3d_sample_slice(mac.ctypes.data, W, H, D, axis, pos, mode, uRef, nu, nv, out.ctypes.data)
+    if rc != 0:
+        raise ValueError("bad slice arguments")
+    return out
+
+
+def advect(mac, W, H, D, seeds, particles, steps, uRef):
+    """The oracle's tracer frame: returns the advected copy of particles (count, 8) float32."""
+    mac = np.ascontiguousarray(mac, dtype=np.float32)
+    seeds = np.ascontiguousarray(seeds, dtype=np.float32)
+    out = np.array(particles, dtype=np.float32, copy=True, order="C")
+    lib().oracle3d_advect(mac.ctypes.data, W, H, D, seeds.ctypes.data, out.ctypes.data, out.size // 8, steps, uRef)
+    return out
 
 
 def decode(f, precision):

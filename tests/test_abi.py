@@ -24,7 +24,7 @@ def test_header_declares_the_solver_api():
     for must in ("cells3d_create", "cells3d_step", "cells3d_read_forces", "cells3d_read_macro", "cells3d_set_sdf",
                  "cells2d_create", "cells2d_step", "cells2d_read_forces", "cells2d_read_macro", "cells2d_set_sdf",
                  "cells2d_update", "cells2d_brush", "cells2d_batch_create", "cells2d_batch_step",
-                 "cells2d_batch_autotune"):
+                 "cells2d_batch_autotune", "cells3d_sample_slice", "cells3d_advect_tracers"):
         assert must in names
 
 

@@ -171,3 +171,22 @@ def test_state_snapshot_round_trip_and_checks():
         t.loadState(bytes(bad))
     s.destroy()
     t.destroy()
+
+
+def test_field_products_check_their_arguments():
+    s = fake(width=12, height=8, depth=6)
+    out = s.sampleSlice(2, 0.5, "vorticity", 0.1)
+    assert out.shape == (8, 12)
+    for bad in (dict(axis=3), dict(pos=1.5), dict(mode="pressure"), dict(uRef=0.0), dict(size=(0, 4))):
+        kw = dict(axis=0, pos=0.5, mode="speed", uRef=0.1, size=None)
+        kw.update(bad)
+        with pytest.raises(_lib.CellsError) as e:
+            s.sampleSlice(**kw)
+        assert e.value.status == _lib.CELLS_E_INVALID
+    parts = np.zeros((4, 8), dtype=np.float32)
+    s.advectTracers(np.zeros((4, 4), dtype=np.float32), parts, 10.0, 0.1)
+    with pytest.raises(_lib.CellsError):
+        s.advectTracers(np.zeros((4, 4), dtype=np.float32), parts, -1.0, 0.1)
+    with pytest.raises(ValueError):
+        s.advectTracers(np.zeros((3, 4), dtype=np.float32), parts, 1.0, 0.1)
+    s.destroy()

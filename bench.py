@@ -134,6 +134,21 @@ def tunnel_setup(W, H, D, precision, device, tau=None, exact=False):
     return s, sdf, macro, tau
 
 
+def copy_roofline(device: int, precision: str, n: int, launches: int = 300, flags: bool = False) -> dict:
+    """The reference's copy roofline (src/bench.ts:61-95) at this size: the 19 population arrays
+    copied between two buffers with no arithmetic, timed with CUDA events; GB/s counts the
+    population bytes (19 loads and 19 stores per cell), as the step's roofline does."""
+    import ctypes as C
+
+    from cells_b200 import _lib
+
+    ms = C.c_double()
+    _lib.check(_lib.lib().cells_copy_roofline(device, _lib.PRECISIONS[precision], 19, n, launches, int(flags),
+                                              C.byref(ms)))
+    gbps = 2 * 19 * _lib.BYTES_PER_POPULATION[_lib.PRECISIONS[precision]] * n / (ms.value * 1e-3) / 1e9
+    return {"ms_per_launch": round(ms.value, 5), "gbps": round(gbps, 1)}
+
+
 def time_steps(s, warmup: int, steps: int):
     s.encodeSteps(warmup)
     s.synchronize()
@@ -321,6 +336,8 @@ def main():
     achieved = per_gpu_mlups * 1e6 * BYTES_PER_CELL[args.precision] / 1e9
     traffic = profiled_traffic(workload)
     info = s.info()
+    copy = copy_roofline(local, args.precision, N)
+    copy["step_frac"] = round(achieved / copy["gbps"], 4)
     line = {
         "metric": METRIC, "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -331,6 +348,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": peak_kind,
                      "bytes_per_cell": BYTES_PER_CELL[args.precision]},
+        "copy_roofline": copy,
         "gpu_launches": launches,
         "clocks": clk,
     }
@@ -351,8 +369,11 @@ def main():
             vms, _ = time_steps(v, 50, 500)
             vn = grid[0] * grid[1] * grid[2]
             vm = vn * 500 / (vms * 1e3)
+            vcopy = copy_roofline(local, prec, vn)
             variants.append({"storage": prec, "grid": list(grid), "mlups": round(vm, 1),
-                             "hbm_frac": round(vm * 1e6 * BYTES_PER_CELL[prec] / 1e9 / hbm, 4)})
+                             "hbm_frac": round(vm * 1e6 * BYTES_PER_CELL[prec] / 1e9 / hbm, 4),
+                             "copy_gbps": vcopy["gbps"],
+                             "copy_frac": round(vm * 1e6 * BYTES_PER_CELL[prec] / 1e9 / vcopy["gbps"], 4)})
             v.destroy()
         line["variants"] = variants
         from cells_b200 import cases2d

@@ -127,6 +127,7 @@ def lib() -> C.CDLL:
         "cells3d_write_populations": (I, [P, P, SZ]),
         "cells3d_read_flags": (I, [P, P, SZ]),
         "cells3d_sample_slice": (I, [P, I, D, I, D, I, I, P]),
+        "cells_copy_roofline": (I, [I, I, I, I64, I, I, C.POINTER(D)]),
         "cells3d_advect_tracers": (I, [P, P, P, I, D, D]),
         "cells3d_timer_start": (I, [P]),
         "cells3d_timer_stop": (I, [P, C.POINTER(C.c_float)]),

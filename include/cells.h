@@ -203,6 +203,16 @@ int cells3d_advect_tracers(Cells3D* h, const float* seeds, float* particles, int
 int cells3d_mass_noalloc(const void* populations, const uint32_t* flags, int64_t n_cells, int32_t precision,
                          double* out_device, void* stream);
 
+/* ---------------- measurement ----------------
+ * copyRoofline (src/bench.ts:61-95): the memory traffic of a step with no arithmetic. Copies q SoA
+ * population arrays of n_cells elements of the precision's storage type between two device
+ * buffers (swapped every launch), 4-byte words per thread (8 for f64), reading one u32 flag word
+ * per word when with_flags is set (the reference's copy reads one per cell); runs `launches`
+ * launches after up to 10 untimed ones and returns the CUDA-event time per launch. Allocates and
+ * frees its own buffers (2 q n_cells bytes-per-element, plus flags). Errors: cells_last_error(NULL). */
+int cells_copy_roofline(int device, int precision, int q, int64_t n_cells, int launches, int with_flags,
+                        double* ms_per_launch);
+
 /* ---------------- discrete adjoint (no counterpart in the reference) ----------------
  * The forward/backward pair of a differentiable run: adjoint_forward steps the solver `steps`
  * steps from its current state (exactly like cells3d_step, plus a checkpoint of the populations

@@ -32,3 +32,10 @@ def test_library_exports_every_declared_symbol():
     lib = ctypes.CDLL(_lib.LIB_PATH)
     missing = [n for n in declared_functions() if not hasattr(lib, n)]
     assert missing == []
+
+
+def test_copy_roofline_rejects_bad_arguments_without_a_device():
+    lib = _lib.lib()
+    ms = ctypes.c_double()
+    for args in ((0, 5, 19, 100, 10, 0), (0, 0, 0, 100, 10, 0), (0, 1, 19, 101, 10, 0), (0, 0, 19, 100, 0, 0)):
+        assert lib.cells_copy_roofline(*args, ctypes.byref(ms)) == _lib.CELLS_E_INVALID

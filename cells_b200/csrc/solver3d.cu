@@ -56,7 +56,9 @@ static void fill_xtab(std::vector<R>& t, int W, double tau, double lambda, doubl
 
 // Interior tile of the step kernel (128 threads per block): 128 cells, or 256 cells as x-pairs for
 // 16-bit storage with an even width. The tile width is workgroup_size when given (the autotuner's
-// knob), else the widest candidate that wastes the fewest threads at the end of a row.
+// knob), else the candidate that wastes the fewest threads at the end of a row: the widest for one
+// cell per thread, the narrowest (64 cells, 32 pairs x 4 rows) for pairs, whose issue-bound kernel
+// gains when more tiles fall wholly outside the absorbing layer and the outlet column.
 void Cells3D::choose_launch() {
   pairTiles = (bpp == 2 && (W % 2) == 0) ? 1 : 0;
   const int cells = pairTiles ? 256 : 128;
@@ -65,7 +67,7 @@ void Cells3D::choose_launch() {
   long long bestWaste = -1;
   for (int c = cells; c >= lo; c >>= 1) {
     const long long waste = (long long)((W + c - 1) / c) * c - W;
-    if (best < 0 || waste < bestWaste) {
+    if (best < 0 || waste < bestWaste || (pairTiles && waste == bestWaste)) {
       best = c;
       bestWaste = waste;
     }
@@ -79,14 +81,23 @@ void Cells3D::choose_launch() {
 }
 
 void Cells3D::upload_xtab() {
+  int firstAbsorb = W;  // the first x with a nonzero absorbing strength
   if (prec == 3) {
     std::vector<double> t;
     fill_xtab<double>(t, W, cfg.tau, lambda_value(), sponge_start(), tau_sponge(), cfg.absorb);
+    for (int x = W - 1; x >= 0; x--)
+      if (t[4 * x + 2] > 0.0) firstAbsorb = x;
     dev.h2d(xTab, t.data(), t.size() * sizeof(double));
   } else {
     std::vector<float> t;
     fill_xtab<float>(t, W, cfg.tau, lambda_value(), sponge_start(), tau_sponge(), cfg.absorb);
+    for (int x = W - 1; x >= 0; x--)
+      if (t[4 * x + 2] > 0.0f) firstAbsorb = x;
     dev.h2d(xTab, t.data(), t.size() * sizeof(float));
+  }
+  if (firstAbsorb != absorbX0) {
+    absorbX0 = firstAbsorb;
+    argGen++;  // step graphs bake the absorbing layer's first x
   }
   if (!dev.fake) dev.sync();  // the host vectors die here
 }
@@ -190,6 +201,7 @@ void Cells3D::enqueue_step_between(const void* src, void* dst, int par, bool sam
   a.tileTX = bx;
   a.tileTY = by;
   a.pairTiles = pairTiles;
+  a.absorbX0 = absorbX0;
   a.nBody = nBody;
   a.rampKind = rampKind;
   a.rampEvery = (int)rampEvery;

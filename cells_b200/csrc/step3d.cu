@@ -64,6 +64,7 @@ struct StepArgs3 {
   int shellBlocks, bodyBlocks;   // block ranges of the face and body roles
   int tileTX, tileTY;            // interior tile: tileTY rows of tileTX cells
   int roleZ;                     // grid z-slices holding the face and body roles
+  int absorbX0;                  // first x of the absorbing layer (W when there is none)
   double rampTarget, rampSteps;
   R lambda, smagC2;
 };
@@ -108,8 +109,10 @@ __device__ __forceinline__ typename C::R feq3s(int i, typename C::R rho, typenam
 //     operations per pair: A = omega+ w e - omega+/2 (fa + fb), B = omega- w rho cu - omega-/2 (fa - fb),
 //     fa' = fa + A + B, fb' = fb + A - B, with e = drho + rho (cu^2/2 - 3u^2/2);
 //   * the absorbing layer depends on x alone, so its branch is taken by whole warps (lanes outside
-//     the layer add sources of zero).
-template <class C, bool SMAG>
+//     the layer add sources of zero);
+//   * ABS = false compiles the collision of a cell outside the absorbing layer with no code for it:
+//     left as a run-time branch, the compiler evaluates the absorbing sources for every cell.
+template <class C, bool SMAG, bool ABS = true>
 __device__ __forceinline__ void collide3(const StepArgs3<C>& a, const typename C::R (&f)[Q3], int x, bool outlet,
                                          typename C::R (&o)[Q3]) {
   using R = typename C::R;
@@ -208,7 +211,7 @@ __device__ __forceinline__ void collide3(const StepArgs3<C>& a, const typename C
     omM = R(1) / (R(0.5) + a.lambda / (R(1) / omP - R(0.5)));
   }
   // absorbing layer: relax toward the inflow equilibrium
-  const bool absorb = kExact ? sigma > R(0) : __any_sync(__activemask(), sigma > R(0));
+  const bool absorb = !ABS ? false : (kExact ? sigma > R(0) : __any_sync(__activemask(), sigma > R(0)));
   R ut = R(0), dq = R(0);
   if (absorb) {
     ut = (R)a.st->uIn[a.par];
@@ -317,11 +320,11 @@ __device__ __forceinline__ void collide3(const StepArgs3<C>& a, const typename C
 }
 
 
-template <class C, bool SMAG>
+template <class C, bool SMAG, bool ABS = true>
 __device__ __forceinline__ void collide_store(const StepArgs3<C>& a, const typename C::R (&f)[Q3], int x, int idx,
                                               bool outlet) {
   typename C::R o[Q3];
-  collide3<C, SMAG>(a, f, x, outlet, o);
+  collide3<C, SMAG, ABS>(a, f, x, outlet, o);
 #pragma unroll
   for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(o[i]);
 }
@@ -561,8 +564,8 @@ __device__ __forceinline__ void body_role(const StepArgs3<C>& a, int bb, int tid
 // directions with c_x = -1, whose source is the copy from (W-2, y, z): a fixed index offset per
 // direction, so all lanes of a warp still issue the same coalesced loads. The inlet cell (x = 0)
 // loads nothing and stores the inflow equilibrium; inlet and outlet stores are short tails, paid
-// once per row.
-template <class C, bool SMAG>
+// once per row. ABS / OUT: the tile overlaps the absorbing layer / holds the outlet column.
+template <class C, bool SMAG, bool ABS, bool OUT>
 __device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int tz) {
   using R = typename C::R;
   const int x = blockIdx.x * a.tileTX + threadIdx.x;
@@ -580,7 +583,7 @@ __device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int tz) {
     for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw((R)eq[i]);
     return;
   }
-  const bool outlet = x == W - 1;
+  const bool outlet = OUT && x == W - 1;
   const long long WH = (long long)W * H;
   R f[Q3];
 #pragma unroll
@@ -590,15 +593,15 @@ __device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int tz) {
     if (cx3(i) == -1 && outlet) e += (int)(-2 + cy3(i) * (long long)W + cz3(i) * WH);
     f[i] = C::raw(a.pull[i] + e);
   }
-  collide_store<C, SMAG>(a, f, x, idx, outlet);
+  collide_store<C, SMAG, ABS>(a, f, x, idx, outlet);
 }
 
 // Interior rows for 16-bit storage (f16, bf16) and an even width: each thread updates the x-pair
 // (x0, x0 + 1), x0 even. One address per population serves both cells; the populations with c_x = 0
 // arrive as one 32-bit load (both cells' values), the others as two 16-bit loads; the 19 results are
 // rounded as a pair and stored with one 32-bit store. Cells of the pair that belong to the body role
-// are left alone.
-template <class C, bool SMAG>
+// are left alone. ABS / OUT: the tile overlaps the absorbing layer / holds the outlet column.
+template <class C, bool SMAG, bool ABS, bool OUT>
 __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
   using R = typename C::R;
   using S = typename C::S;
@@ -616,7 +619,7 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
     if (!act0 && !act1) return;
   }
   const bool inlet0 = x0 == 0;
-  const bool outlet1 = x0 + 1 == W - 1;
+  const bool outlet1 = OUT && x0 + 1 == W - 1;
   const long long WH = (long long)W * H;
   uint32_t r[Q3];  // populations of the pair: x0 in the low half, x0 + 1 in the high half
 #pragma unroll
@@ -644,7 +647,7 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
       R f[Q3];
 #pragma unroll
       for (int i = 0; i < Q3; i++) f[i] = C::lo(r[i]);
-      collide3<C, SMAG>(a, f, x0, false, o0);
+      collide3<C, SMAG, ABS>(a, f, x0, false, o0);
     }
   }
   R o1[Q3];
@@ -652,7 +655,7 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
     R f[Q3];
 #pragma unroll
     for (int i = 0; i < Q3; i++) f[i] = C::hi(r[i]);
-    collide3<C, SMAG>(a, f, x0 + 1, outlet1, o1);
+    collide3<C, SMAG, ABS>(a, f, x0 + 1, outlet1, o1);
   }
   if (act0 && act1) {
 #pragma unroll
@@ -697,10 +700,21 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<C>(PAIR))
       body_role<C, SMAG>(a, r - a.shellBlocks, tid);
     return;
   }
-  if constexpr (PAIR)
-    bulk_pair_role<C, SMAG>(a, blockIdx.z - a.roleZ);
-  else
-    bulk_role<C, SMAG>(a, blockIdx.z - a.roleZ);
+  // block-uniform choice of the code for tiles that overlap the absorbing layer or hold the outlet
+  const int tx1 = (blockIdx.x + 1) * a.tileTX;  // end of the tile's x range
+  const bool abs = tx1 > a.absorbX0, out = tx1 >= a.W;
+  const int tz = blockIdx.z - a.roleZ;
+  if constexpr (PAIR) {
+    if (out)
+      abs ? bulk_pair_role<C, SMAG, true, true>(a, tz) : bulk_pair_role<C, SMAG, false, true>(a, tz);
+    else
+      abs ? bulk_pair_role<C, SMAG, true, false>(a, tz) : bulk_pair_role<C, SMAG, false, false>(a, tz);
+  } else {
+    if (out)
+      abs ? bulk_role<C, SMAG, true, true>(a, tz) : bulk_role<C, SMAG, false, true>(a, tz);
+    else
+      abs ? bulk_role<C, SMAG, true, false>(a, tz) : bulk_role<C, SMAG, false, false>(a, tz);
+  }
 }
 
 // ---------------- host-side launcher ----------------
@@ -740,6 +754,7 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   a.rampSteps = L.rampSteps;
   a.lambda = (R)L.lambda;
   a.smagC2 = (R)L.smagC2;
+  a.absorbX0 = L.absorbX0;
   // work split
   const long long nShell = shell_cells3(L.W, L.H, L.D);
   a.shellBlocks = (int)((nShell + kStepThreads - 1) / kStepThreads);

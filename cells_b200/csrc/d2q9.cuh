@@ -76,6 +76,11 @@ struct Tunnel2 {
   double2* partials;      // one force partial per tile
   double2* history;       // HISTORY2_LEN force samples
   DevState2* st;
+  // per x, in the arithmetic type (float4 or double4): omega+ without Smagorinsky (the sponge's
+  // 1 / mix(tau, tauSponge, sOut)), omega- for that omega+, the absorbing strength sigma, and
+  // 1 / omega+ -- filled on the host with the kernel's own expressions (src/shaders/step.ts:48-63,
+  // :215-223), so the step reads them instead of evaluating two smoothsteps and four divisions per cell
+  const void* xtab;
   int W, H;
   int tilesX, nTiles;     // tiles of this tunnel (tile = one block's cells)
   int firstTile;          // index of its first tile in the batch

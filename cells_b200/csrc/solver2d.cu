@@ -44,6 +44,7 @@ struct Tunnel2Host {
   int partialsCap = 0;
   double2* history = nullptr;
   DevState2* st = nullptr;
+  void* xtab = nullptr;  // W entries of 4 values in the arithmetic type (Tunnel2::xtab)
   int tilesX = 0, nTiles = 0, firstTile = 0;
 
   // host bookkeeping (src/solver.ts:57-61)
@@ -185,6 +186,36 @@ void Cells2DBatch::set_layout(int tx, int ty, int pers) {
   layoutGen++;
 }
 
+// The per-x rates of a tunnel (Tunnel2::xtab) in the arithmetic type R, by the step kernel's
+// expressions for the sponge, inlet layer and TRT rates (src/shaders/step.ts:48-63, :215-223) in the
+// same operation order, so the values equal what the kernel computed per cell before.
+template <class R>
+static void fill_xtab2(std::vector<R>& t, int W, const double* p) {
+  const R tau = (R)p[P2_TAU], lam = (R)p[P2_LAMBDA], ss = (R)p[P2_SPONGE_START], ts = (R)p[P2_TAU_SPONGE];
+  const R ab = (R)p[P2_ABSORB], il = (R)p[P2_INLET_LAYER];
+  auto smooth = [](R e0, R e1, R x) {
+    R u = (x - e0) / (e1 - e0);
+    u = u < R(0) ? R(0) : (R(1) < u ? R(1) : u);
+    return u * u * (R(3) - R(2) * u);
+  };
+  t.assign((size_t)W * 4, R(0));
+  for (int x = 0; x < W; x++) {
+    R omegaBase = R(1) / tau;
+    R sOut = R(0);
+    if (ss < R(W - 1)) {
+      sOut = smooth(ss, R(W - 1), R(x));
+      omegaBase = R(1) / (tau * (R(1) - sOut) + ts * sOut);
+    }
+    R sIn = R(0);
+    if (il > R(0)) sIn = R(1) - smooth(R(0), il, R(x));
+    const R sOut2 = sOut * sOut, sIn2 = sIn * sIn;
+    t[4 * (size_t)x] = omegaBase;
+    t[4 * (size_t)x + 1] = R(1) / (R(0.5) + lam / (R(1) / omegaBase - R(0.5)));
+    t[4 * (size_t)x + 2] = ab * (sOut2 < sIn2 ? sIn2 : sOut2);
+    t[4 * (size_t)x + 3] = R(1) / omegaBase;
+  }
+}
+
 // The tunnel's descriptor, with every parameter derived as writeParams does (src/solver.ts:180-197)
 // and rounded once into f32 (and kept in f64 for f64 arithmetic).
 void Cells2DBatch::upload_tunnel(int k) {
@@ -198,6 +229,7 @@ void Cells2DBatch::upload_tunnel(int k) {
   d.partials = T.partials;
   d.history = T.history;
   d.st = T.st;
+  d.xtab = T.xtab;
   d.W = T.W;
   d.H = T.H;
   d.tilesX = T.tilesX;
@@ -229,9 +261,18 @@ void Cells2DBatch::upload_tunnel(int k) {
     d.pf[i] = (float)p[i];
     d.pd[i] = p[i];
   }
+  std::vector<float> tf;
+  std::vector<double> td;
+  if (prec == CELLS_FP64) {
+    fill_xtab2<double>(td, T.W, p);
+    dev.h2d(T.xtab, td.data(), td.size() * sizeof(double));
+  } else {
+    fill_xtab2<float>(tf, T.W, p);
+    dev.h2d(T.xtab, tf.data(), tf.size() * sizeof(float));
+  }
   if (dev.fake) return;
   dev.h2d(dTunnels + k, &d, sizeof(d));
-  dev.sync();  // d dies here
+  dev.sync();  // d and the tables die here
 }
 
 void Cells2DBatch::write_state(int k, int which) {
@@ -434,8 +475,12 @@ static Cells2DBatch* create_batch(const Cells2DConfig* cfgs, int count) {
     for (int k = 0; k < count; k++) {
       Tunnel2Host& T = b->t[(size_t)k];
       const size_t fBytes = 9ull * b->bpp * (size_t)T.N;
-      T.f[0] = b->dev.alloc(fBytes, "distribution buffer A");
-      T.f[1] = b->dev.alloc(fBytes, "distribution buffer B");
+      // the step kernel issues every cell's nine fast-path pulls before it knows whether the cell
+      // takes them; on the top row direction 8's pull lands up to W - 1 elements past the nine
+      // arrays, so each buffer carries W elements of padding (never used as a population)
+      const size_t padBytes = (size_t)T.W * b->bpp;
+      T.f[0] = b->dev.alloc(fBytes + padBytes, "distribution buffer A");
+      T.f[1] = b->dev.alloc(fBytes + padBytes, "distribution buffer B");
       T.flags = (uint32_t*)b->dev.alloc((size_t)T.N * 4, "flags");
       T.sdf = (float*)b->dev.alloc((size_t)T.N * 4, "sdf");
       T.macro = (float4*)b->dev.alloc((size_t)T.N * 16, "macro");
@@ -445,11 +490,12 @@ static Cells2DBatch* create_batch(const Cells2DConfig* cfgs, int count) {
       T.partials = (double2*)b->dev.alloc((size_t)cap * sizeof(double2), "force partials");
       T.history = (double2*)b->dev.alloc((size_t)HISTORY2_LEN * sizeof(double2), "force history");
       T.st = (DevState2*)b->dev.alloc(sizeof(DevState2), "state");
+      T.xtab = b->dev.alloc((size_t)T.W * 4 * b->bpp, "x table");
       T.stageHist = (double2*)b->dev.host_pinned((size_t)HISTORY2_LEN * sizeof(double2));
       T.stageState = (unsigned*)b->dev.host_pinned(64);
       b->dev.memset0(T.st, sizeof(DevState2));
-      b->dev.memset0(T.f[0], fBytes);
-      b->dev.memset0(T.f[1], fBytes);
+      b->dev.memset0(T.f[0], fBytes + padBytes);
+      b->dev.memset0(T.f[1], fBytes + padBytes);
       b->dev.memset0(T.flags, (size_t)T.N * 4);
       std::vector<float> far((size_t)T.N, 1e6f);  // src/solver.ts:133
       b->dev.h2d(T.sdf, far.data(), far.size() * 4);

@@ -20,8 +20,10 @@
 
 #ifdef CELLS_EXACT_ARITH
 #define CELLS_NS exact
+constexpr bool kExact2 = true;
 #else
 #define CELLS_NS fast
+constexpr bool kExact2 = false;
 #endif
 
 namespace cells {
@@ -57,16 +59,25 @@ template <class R>
 __device__ __forceinline__ R clampR(R v, R lo, R hi) {
   return v < lo ? lo : (hi < v ? hi : v);
 }
-// WGSL smoothstep(e0, e1, x) and mix(a, b, t)
+// 1 / v: IEEE in the exact build and for f64; the hardware reciprocal (within 2 ulp, no branch)
+// for f32 in the fast build
 template <class R>
-__device__ __forceinline__ R smoothstepR(R e0, R e1, R x) {
-  R t = clampR<R>((x - e0) / (e1 - e0), R(0), R(1));
-  return t * t * (R(3) - R(2) * t);
+__device__ __forceinline__ R recip2(R v) {
+  if constexpr (!kExact2 && sizeof(R) == 4)
+    return __fdividef(R(1), v);
+  else
+    return R(1) / v;
 }
 template <class R>
-__device__ __forceinline__ R mixR(R a, R b, R t) {
-  return a * (R(1) - t) + b * t;
-}
+struct XTab2;
+template <>
+struct XTab2<float> {
+  using T = float4;
+};
+template <>
+struct XTab2<double> {
+  using T = double4;
+};
 
 struct Geo2 {
   int W, H;
@@ -143,37 +154,54 @@ __device__ __forceinline__ typename C::R pull_slow2(int i, const Geo2& g, const 
   return (R)C::ld(&src[j * N + idx]);
 }
 
-// main, src/shaders/step.ts:177-227, for the cell (x, y) of tunnel T. Returns whether the cell has
-// a force slot (its force is then in force[0..1]).
+// The fields of a tunnel that every cell of a tile reads, loaded once per thread.
 template <class C>
-__device__ __forceinline__ bool cell2(const Tunnel2& T, int par, typename C::R uIn, int x, int y,
+struct Hot2 {
+  const typename C::S* __restrict__ src;
+  typename C::S* __restrict__ dst;
+  const uint32_t* __restrict__ flags;
+  const typename XTab2<typename C::R>::T* __restrict__ xtab;
+  int W, H, N;
+  int forcing;
+  typename C::R smagC2;
+};
+
+// main, src/shaders/step.ts:177-227, for the cell (x, y) of tunnel T. Returns whether the cell has
+// a force slot (its force is then in force[0..1]). The x-dependent rates come from the tunnel's x
+// table; the exact build evaluates every other expression in the reference's order.
+template <class C>
+__device__ __forceinline__ bool cell2(const Tunnel2& T, const Hot2<C>& h, typename C::R uIn, int x, int y,
                                       typename C::R force[2]) {
   using R = typename C::R;
   using S = typename C::S;
-  Geo2 g;
-  g.W = T.W;
-  g.H = T.H;
-  g.left = T.left;
-  g.right = T.right;
-  g.bottom = T.bottom;
-  g.top = T.top;
-  const long long N = (long long)g.W * g.H;
-  const S* __restrict__ src = (const S*)T.f[par];
-  S* __restrict__ dst = (S*)T.f[par ^ 1];
-  const uint32_t* __restrict__ flags = T.flags;
-  const long long idx = (long long)y * g.W + x;
-  const uint32_t fl = __ldg(&flags[idx]);
+  const int W = h.W;
+  const int N = h.N;  // 9 N < 2^31: checked when the tunnel is created
+  const S* __restrict__ src = h.src;
+  S* __restrict__ dst = h.dst;
+  const int idx = y * W + x;
+  const uint32_t fl = __ldg(&h.flags[idx]);
+  // the fast path's nine pulls go out together with the flag load (one memory round trip per cell,
+  // not two); a flagged cell replaces them below. Every address is inside the allocation: the
+  // largest, direction 8 on the top row, is at most W - 1 elements past the nine arrays, which the
+  // host pads.
   R f[Q2];
-  bool slot = false;
-  if (fl == 0u) {
 #pragma unroll
-    for (int i = 0; i < Q2; i++) f[i] = (R)C::ld(&src[i * N + idx - (long long)cy2(i) * g.W - cx2(i)]);
-  } else {
+  for (int i = 0; i < Q2; i++) f[i] = (R)C::ld(src + (i * N + idx - cy2(i) * W - cx2(i)));
+  bool slot = false;
+  if (fl != 0u) {
     if (fl & FLAG2_SOLID) return false;
+    Geo2 g;
+    g.W = W;
+    g.H = h.H;
+    g.left = T.left;
+    g.right = T.right;
+    g.bottom = T.bottom;
+    g.top = T.top;
     const R uLid = prm<R>(T, P2_ULID);
     f[0] = (R)C::ld(&src[idx]);
 #pragma unroll
-    for (int i = 1; i < Q2; i++) f[i] = pull_slow2<C>(i, g, src, flags, T.sdf, N, x, y, idx, fl, uLid, force);
+    for (int i = 1; i < Q2; i++)
+      f[i] = pull_slow2<C>(i, g, src, h.flags, T.sdf, (long long)N, x, y, (long long)idx, fl, uLid, force);
     slot = (fl >> BIDX2_SHIFT) != 0u;
     // Zou-He (populations stored shifted by w_i)
     if (fl & FLAG2_INLET) {
@@ -192,10 +220,10 @@ __device__ __forceinline__ bool cell2(const Tunnel2& T, int par, typename C::R u
   // moments (src/shaders/step.ts:22-32)
   const R drho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
   const R rho = R(1) + drho;
-  const R invRho = R(1) / rho;
+  const R invRho = recip2<R>(rho);
   R ux = (f[1] - f[3] + f[5] - f[6] - f[7] + f[8]) * invRho;
   R uy = (f[2] - f[4] + f[5] + f[6] - f[7] - f[8]) * invRho;
-  const int forcing = T.forcing;
+  const int forcing = h.forcing;
   R bfx = R(0), bfy = R(0);
   if (forcing != 0) {
     bfx = prm<R>(T, P2_FX);
@@ -215,24 +243,13 @@ __device__ __forceinline__ bool cell2(const Tunnel2& T, int par, typename C::R u
     eqS[a] = w2<R>(a) * (drho + rho * (R(0.5) * cu[a] * cu[a] - usq));
     eqA[a] = w2<R>(a) * rho * cu[a];
   }
-  // sponge and absorbing layers (src/shaders/step.ts:215-223)
-  const R tau = prm<R>(T, P2_TAU);
-  const R spongeStart = prm<R>(T, P2_SPONGE_START);
-  R omegaBase = R(1) / tau;
-  R sOut = R(0);
-  if (spongeStart < R(g.W - 1)) {
-    sOut = smoothstepR<R>(spongeStart, R(g.W - 1), R(x));
-    omegaBase = R(1) / mixR<R>(tau, prm<R>(T, P2_TAU_SPONGE), sOut);
-  }
-  R sIn = R(0);
-  const R inletLayer = prm<R>(T, P2_INLET_LAYER);
-  if (inletLayer > R(0)) sIn = R(1) - smoothstepR<R>(R(0), inletLayer, R(x));
-  const R sOut2 = sOut * sOut, sIn2 = sIn * sIn;
-  const R sigma = prm<R>(T, P2_ABSORB) * (sOut2 < sIn2 ? sIn2 : sOut2);
+  // sponge and absorbing layers (src/shaders/step.ts:215-223), from the x table
+  const auto xt = h.xtab[x];  // read-only for the whole launch
+  const R omegaBase = xt.x;
+  const R sigma = xt.z;
   // Smagorinsky (src/shaders/step.ts:48-63)
-  R omP = omegaBase;
-  const R smagC2 = prm<R>(T, P2_SMAGC2);
-  if (smagC2 > R(0)) {
+  R omP = omegaBase, omM = xt.y;
+  if (h.smagC2 > R(0)) {
     R n[Q2];
 #pragma unroll
     for (int a : {1, 2, 5, 6}) {
@@ -244,11 +261,13 @@ __device__ __forceinline__ bool cell2(const Tunnel2& T, int par, typename C::R u
     const R pyy = n[2] + n[4] + n[5] + n[6] + n[7] + n[8];
     const R pxy = n[5] - n[6] + n[7] - n[8];
     const R pi = sqrt(pxx * pxx + pyy * pyy + R(2) * pxy * pxy);
-    const R t0 = R(1) / omegaBase;
-    const R tEff = R(0.5) * (t0 + sqrt(t0 * t0 + (R)25.45584412271571 * smagC2 * pi * invRho));
-    omP = R(1) / tEff;
+    const R t0 = xt.w;  // 1 / omegaBase
+    const R tEff = R(0.5) * (t0 + sqrt(t0 * t0 + (R)25.45584412271571 * h.smagC2 * pi * invRho));
+    omP = recip2<R>(tEff);
+    // the exact build divides 1 by omega+ again, as the reference does; the fast build uses tEff
+    const R tP = kExact2 ? R(1) / omP : tEff;
+    omM = recip2<R>(R(0.5) + prm<R>(T, P2_LAMBDA) / (tP - R(0.5)));
   }
-  const R omM = R(1) / (R(0.5) + prm<R>(T, P2_LAMBDA) / (R(1) / omP - R(0.5)));
   // absorbing-layer and Guo body-force sources (src/shaders/step.ts:65-91)
   R s0 = R(0);
   R sS[Q2], sA[Q2];
@@ -258,7 +277,7 @@ __device__ __forceinline__ bool cell2(const Tunnel2& T, int par, typename C::R u
     sA[a] = R(0);
   }
   if (sigma > R(0)) {
-    const R ut = inlet_velocity2<R>(T.parabolic, uIn, g.H, y);
+    const R ut = inlet_velocity2<R>(T.parabolic, uIn, h.H, y);
     const R dq = R(1.5) * rho * (ut * ut - ux * ux - uy * uy);
     s0 += sigma * w2<R>(0) * -dq;
 #pragma unroll
@@ -324,7 +343,19 @@ __device__ __forceinline__ void tile2(const Tunnel2* __restrict__ tunnels, int t
   }
   R force[2] = {R(0), R(0)};
   bool slot = false;
-  if (x < T.W && y < T.H) slot = cell2<C>(T, par, (R)uInD, x, y, force);
+  if (x < T.W && y < T.H) {
+    Hot2<C> h;
+    h.W = T.W;
+    h.H = T.H;
+    h.N = h.W * h.H;
+    h.src = (const typename C::S*)T.f[par];
+    h.dst = (typename C::S*)T.f[par ^ 1];
+    h.flags = T.flags;
+    h.xtab = (const typename XTab2<R>::T*)T.xtab;
+    h.forcing = T.forcing;
+    h.smagC2 = prm<R>(T, P2_SMAGC2);
+    slot = cell2<C>(T, h, (R)uInD, x, y, force);
+  }
   if (!sample) return;
   // f64 sum of the tile's forces: warp shuffles, then warps in order
   if (__syncthreads_or(slot ? 1 : 0)) {
@@ -384,8 +415,16 @@ __device__ __forceinline__ void tile2(const Tunnel2* __restrict__ tunnels, int t
   }
 }
 
+// The f32 kernel is latency-bound: capped at 64 registers (4 blocks of 256 threads per SM) it keeps
+// more warps resident, which measured faster than its natural 76-80 registers despite a few spilled
+// words; the f64 kernel keeps its registers.
 template <class C>
-__global__ void __launch_bounds__(256) step2d_kernel(const Tunnel2* __restrict__ tunnels,
+constexpr int min_blocks2() {
+  return sizeof(typename C::R) == 4 ? 4 : 1;
+}
+
+template <class C>
+__global__ void __launch_bounds__(256, min_blocks2<C>()) step2d_kernel(const Tunnel2* __restrict__ tunnels,
                                                      const unsigned short* __restrict__ tileTunnel, int par,
                                                      int allowSample) {
   const int b = blockIdx.x;
@@ -424,7 +463,7 @@ __device__ __forceinline__ bool grid_barrier2(unsigned* counter, unsigned target
 // nSteps steps of every tunnel in one launch: each resident block walks the tiles with a grid
 // stride, then all blocks meet at the barrier before the next step.
 template <class C>
-__global__ void __launch_bounds__(256) step2d_persistent_kernel(const Tunnel2* __restrict__ tunnels,
+__global__ void __launch_bounds__(256, min_blocks2<C>()) step2d_persistent_kernel(const Tunnel2* __restrict__ tunnels,
                                                                 const unsigned short* __restrict__ tileTunnel,
                                                                 int nTiles, int par, int nSteps, int allowSample,
                                                                 unsigned* barrier, int* error) {

@@ -170,16 +170,24 @@ __global__ void __launch_bounds__(kAdjThreads) adj_cells3_kernel(AdjLaunch3 a) {
   R* __restrict__ lamOut = (R*)a.lamOut;
   double du = 0.0;
   const int idx = x + W * (y + H * (int)blockIdx.z);
-  const uint32_t fl = (x < W && y < H) ? __ldg(&a.flags[idx]) : FLAG3_SOLID;
-  if (fl == 0u) {
-    // interior cell: plain pulls, the collision's transposed Jacobian, plain pushes
-    R g[Q3], lp[Q3], lg[Q3];
+  const bool in = x < W && y < H;
+  // the plain pulls and lambda^{n+1} go out with the flag load rather than after it: for every cell
+  // of the grid each address lies inside the 19 N arrays (no D3Q19 direction reaches further than
+  // one plane, and the arrays of directions 1 and 18 are not the first and last), and flagged cells
+  // discard the values
+  R g[Q3], lp[Q3];
+  if (in) {
 #pragma unroll
     for (int i = 0; i < Q3; i++) {
       const int o = i * N + idx;
       lp[i] = __ldg(&lamNext[o]);
       g[i] = __ldg(&f[o - (int)off3(i, W, H)]);
     }
+  }
+  const uint32_t fl = in ? __ldg(&a.flags[idx]) : FLAG3_SOLID;
+  if (fl == 0u) {
+    // interior cell: plain pulls, the collision's transposed Jacobian, plain pushes
+    R lg[Q3];
     const R* xt = (const R*)a.xTab + 4 * x;
     R dut = R(0);
     collide_adjoint3<R>(g, lp, xt[0], xt[1], xt[2], (R)__ldg(&a.uDev[adj_step(a)]), lg, dut);

@@ -575,16 +575,10 @@ __device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int tz) {
   if (x >= W || y >= H - 1) return;
   const int row = y + H * z;
   const int idx = x + W * row;
-  if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
-  if (x == 0) {
-    // inlet: equilibrium at the inflow speed, no collision (step3d.ts:190-193)
-    const double* eq = a.st->inletEq[a.par];
-#pragma unroll
-    for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw((R)eq[i]);
-    return;
-  }
   const bool outlet = OUT && x == W - 1;
   const long long WH = (long long)W * H;
+  // the pulls go out before the body-row and inlet tests, so they do not wait for them (every
+  // interior pull address is inside the grid; body and inlet cells discard them)
   R f[Q3];
 #pragma unroll
   for (int i = 0; i < Q3; i++) {
@@ -592,6 +586,14 @@ __device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int tz) {
     // outlet: zero-gradient copy from (W-2, y, z) for the directions entering through x = W-1
     if (cx3(i) == -1 && outlet) e += (int)(-2 + cy3(i) * (long long)W + cz3(i) * WH);
     f[i] = C::raw(a.pull[i] + e);
+  }
+  if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
+  if (x == 0) {
+    // inlet: equilibrium at the inflow speed, no collision (step3d.ts:190-193)
+    const double* eq = a.st->inletEq[a.par];
+#pragma unroll
+    for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw((R)eq[i]);
+    return;
   }
   collide_store<C, SMAG, ABS>(a, f, x, idx, outlet);
 }
@@ -612,15 +614,11 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
   if (x0 >= W || y >= H - 1) return;
   const int row = y + H * z;
   const int idx = x0 + W * row;
-  bool act0 = true, act1 = true;
-  if (a.rowBody[row]) {
-    act0 = __ldg(a.flags + idx) == 0u;
-    act1 = __ldg(a.flags + idx + 1) == 0u;
-    if (!act0 && !act1) return;
-  }
   const bool inlet0 = x0 == 0;
   const bool outlet1 = OUT && x0 + 1 == W - 1;
   const long long WH = (long long)W * H;
+  // the pulls go out before the body-row test, so they do not wait for it (every interior pull
+  // address is inside the grid; a pair of body cells discards them)
   uint32_t r[Q3];  // populations of the pair: x0 in the low half, x0 + 1 in the high half
 #pragma unroll
   for (int i = 0; i < Q3; i++) {
@@ -635,6 +633,12 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
       const uint32_t v1 = __ldg(reinterpret_cast<const unsigned short*>(p + e1));
       r[i] = v0 | (v1 << 16);
     }
+  }
+  bool act0 = true, act1 = true;
+  if (a.rowBody[row]) {
+    act0 = __ldg(a.flags + idx) == 0u;
+    act1 = __ldg(a.flags + idx + 1) == 0u;
+    if (!act0 && !act1) return;
   }
   R o0[Q3];
   if (act0) {

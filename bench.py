@@ -284,7 +284,26 @@ def main():
     ap.add_argument("--grid", default="192x96x96")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, variants and the CPU baseline")
     ap.add_argument("--profile", action="store_true", help="short run for ncu: warmup + steps only, no extras")
+    ap.add_argument("--profile2d", action="store_true",
+                    help="short run for ncu of the 2D step kernel: the 64 batched NACA tunnels, one launch per "
+                         "step (tile 32 x 2), warmup + steps")
     args = ap.parse_args()
+    if args.profile2d:
+        from cells_b200 import cases2d
+        from cells_b200.rng import perturbed_rest2
+        from cells_b200.solver2d import Batch2D
+
+        tunnels = cases2d.batched_naca_tunnels(64)
+        b = Batch2D([dict(c, device=0) for c, _ in tunnels])
+        for t, (c, sdf) in zip(b.tunnels, tunnels):
+            t.setSdf(sdf)
+            t.initField(perturbed_rest2(c["width"], c["height"], 1e-4))
+        b.setLaunch(32, 2, False)
+        b.step(max(3, args.warmup) + args.steps)
+        b.synchronize()
+        b.destroy()
+        print(json.dumps({"profile2d": "done", "steps": max(3, args.warmup) + args.steps}))
+        return
     W, H, D = (int(v) for v in args.grid.lower().split("x"))
     N = W * H * D
     world = int(os.environ.get("WORLD_SIZE", "1"))

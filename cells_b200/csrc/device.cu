@@ -41,6 +41,12 @@ void Device::close() {
     return;
   }
   if (stream) cudaStreamSynchronize(stream);
+  for (int b = 0; b < 2; b++) {
+    if (stage[b]) cudaFreeHost(stage[b]);
+    if (stageEv[b]) cudaEventDestroy(stageEv[b]);
+    stage[b] = nullptr;
+    stageEv[b] = nullptr;
+  }
   for (void* p : owned) cudaFree(p);
   owned.clear();
   if (ev0) cudaEventDestroy(ev0);
@@ -79,6 +85,37 @@ void Device::h2d(void* d, const void* h, size_t bytes) {
     return;
   }
   check_cuda(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync H2D");
+}
+
+constexpr size_t kStageBytes = 2u << 20;
+
+void Device::d2h_large(void* h, const void* d, size_t bytes) {
+  if (fake || bytes < 2 * kStageBytes) {
+    d2h(h, d, bytes);
+    sync();
+    return;
+  }
+  if (!stage[0]) {
+    for (int b = 0; b < 2; b++) {
+      check_cuda(cudaMallocHost(&stage[b], kStageBytes), "cudaMallocHost");
+      check_cuda(cudaEventCreateWithFlags(&stageEv[b], cudaEventDisableTiming), "cudaEventCreate");
+    }
+  }
+  const size_t chunks = (bytes + kStageBytes - 1) / kStageBytes;
+  auto issue = [&](size_t k) {
+    const size_t off = k * kStageBytes, n = bytes - off < kStageBytes ? bytes - off : kStageBytes;
+    check_cuda(cudaMemcpyAsync(stage[k & 1], (const char*)d + off, n, cudaMemcpyDeviceToHost, stream),
+               "cudaMemcpyAsync D2H");
+    check_cuda(cudaEventRecord(stageEv[k & 1], stream), "cudaEventRecord");
+  };
+  issue(0);
+  issue(1);
+  for (size_t k = 0; k < chunks; k++) {
+    const size_t off = k * kStageBytes, n = bytes - off < kStageBytes ? bytes - off : kStageBytes;
+    check_cuda(cudaEventSynchronize(stageEv[k & 1]), "cudaEventSynchronize");
+    std::memcpy((char*)h + off, stage[k & 1], n);
+    if (k + 2 < chunks) issue(k + 2);  // the buffer is free again: its chunk has been copied out
+  }
 }
 
 void Device::d2h(void* h, const void* d, size_t bytes) {

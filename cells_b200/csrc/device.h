@@ -41,6 +41,13 @@ struct Device {
   void* alloc(size_t bytes, const char* what);
   void h2d(void* d, const void* h, size_t bytes);
   void d2h(void* h, const void* d, size_t bytes);
+  // Device-to-host copy of a large buffer into pageable memory, waiting for it: through two pinned
+  // 2 MiB buffers (allocated on first use, freed by close), the copy of chunk k out of one overlapping
+  // the DMA of chunk k + 1 into the other. A pageable destination otherwise runs at a fraction of the
+  // pinned rate. Small copies take d2h and a sync.
+  void d2h_large(void* h, const void* d, size_t bytes);
+  void* stage[2] = {nullptr, nullptr};
+  cudaEvent_t stageEv[2] = {nullptr, nullptr};
   void memset0(void* d, size_t bytes);
   void sync();
   void* host_pinned(size_t bytes);

@@ -122,8 +122,7 @@ void Cells3D::build_body_list(const std::vector<uint8_t>& rows) {
   std::vector<int> cells;
   if (!dev.fake) {
     std::vector<uint32_t> fl((size_t)N);
-    dev.d2h(fl.data(), flags, (size_t)N * 4);
-    dev.sync();
+    dev.d2h_large(fl.data(), flags, (size_t)N * 4);
     for (int z = 0; z < D; z++)
       for (int y = 0; y < H; y++) {
         if (!rows[(size_t)y + (size_t)H * z]) continue;
@@ -586,8 +585,7 @@ int cells3d_synchronize(Cells3D* h) {
 int cells3d_read_macro(Cells3D* h, float* out4n) {
   if (!h || !out4n) return CELLS_E_INVALID;
   CELLS_TRY(h)
-  h->dev.d2h(out4n, h->macro, (size_t)h->N * 16);
-  h->dev.sync();
+  h->dev.d2h_large(out4n, h->macro, (size_t)h->N * 16);
   CELLS_CATCH(h)
 }
 

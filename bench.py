@@ -284,10 +284,25 @@ def main():
     ap.add_argument("--grid", default="192x96x96")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, variants and the CPU baseline")
     ap.add_argument("--profile", action="store_true", help="short run for ncu: warmup + steps only, no extras")
+    ap.add_argument("--profile-adjoint", action="store_true",
+                    help="short run for ncu of the discrete adjoint: the 128x64x64 star body over --steps steps "
+                         "(checkpoints every 100), forward then backward sweep")
     ap.add_argument("--profile2d", action="store_true",
                     help="short run for ncu of the 2D step kernel: the 64 batched NACA tunnels, one launch per "
                          "step (tile 32 x 2), warmup + steps")
     args = ap.parse_args()
+    if args.profile_adjoint:
+        from cells_b200.adjoint import StarDrag
+        from cells_b200.rng import SEED, normal
+
+        n = max(200, (args.steps // 100) * 100)
+        p = StarDrag(precision="fp32", device=0, steps=n, ramp_steps=n // 2, window=(n // 2, n))
+        J = p.forward(0.02 * normal(SEED, 17, 16))
+        p.backward()
+        p.solver.synchronize()
+        p.destroy()
+        print(json.dumps({"profile_adjoint": "done", "steps": n, "J": J}))
+        return
     if args.profile2d:
         from cells_b200 import cases2d
         from cells_b200.rng import perturbed_rest2

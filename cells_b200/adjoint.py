@@ -84,10 +84,15 @@ class StarDrag:
         return np.stack([-self.r0 * g.real_sph_harm(l, m, theta, phi) for l, m in g.SH_INDEX], axis=1)
 
     def backward(self):
-        """(dJ/dcoef (16,), dJ/du) of the last forward."""
+        """(dJ/dcoef (16,), dJ/du) of the last forward: the adjoint sweep, then the host chain rule."""
         if self._J is None:
             raise RuntimeError("backward needs a forward first")
-        r = self.solver.adjointBackward()
+        return self.coefficient_gradient(self.solver.adjointBackward())
+
+    def coefficient_gradient(self, r):
+        """(dJ/dcoef (16,), dJ/du) from the sweep's result r (Solver3D.adjointBackward): dJ/dsdf times
+        the SDF's derivative by the coefficients at the nodes the gradient touches, and dJ/du with the
+        coefficient scale's own dependence on u."""
         dsdf = r["dsdf"]
         nodes = np.flatnonzero(dsdf)
         dcoef = dsdf[nodes] @ self.sdf_jacobian_nodes(nodes) if nodes.size else np.zeros(16)

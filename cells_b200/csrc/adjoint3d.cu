@@ -38,14 +38,20 @@ struct XRow {
 
 // (dC/dg)^T lp for the TRT collision with sponge rate omP/omM and absorbing strength sigma toward
 // the inflow speed ut (src/shaders/step3d.ts:38-102, Smagorinsky off). Also returns dJ/dut.
-template <class R>
+// ABS = false: a cell known to lie outside the absorbing layer, compiled without its terms (as a
+// run-time branch the compiler evaluates them for every cell). f32 takes the hardware reciprocal.
+template <class R, bool ABS = true>
 __device__ __forceinline__ void collide_adjoint3(const R g[Q3], const R lp[Q3], R omP, R omM, R sigma, R ut,
                                                  R lg[Q3], R& dut) {
   R drho = R(0);
 #pragma unroll
   for (int i = 0; i < Q3; i++) drho += g[i];
   const R rho = R(1) + drho;
-  const R inv = R(1) / rho;
+  R inv;
+  if constexpr (sizeof(R) == 4)
+    inv = __fdividef(R(1), rho);
+  else
+    inv = R(1) / rho;
   R jx = R(0), jy = R(0), jz = R(0);
 #pragma unroll
   for (int i = 1; i < Q3; i++) {
@@ -64,7 +70,7 @@ __device__ __forceinline__ void collide_adjoint3(const R g[Q3], const R lp[Q3], 
     rhoB += e0 * w0 * (R(1) - usq);
     usqB -= e0 * w0 * rho;
   }
-  const bool absorb = sigma > R(0);
+  const bool absorb = ABS && sigma > R(0);
   if (absorb) dqB -= lp[0] * sigma * w0;
 #pragma unroll
   for (int a = 1; a < Q3; a += 2) {
@@ -190,7 +196,11 @@ __global__ void __launch_bounds__(kAdjThreads) adj_cells3_kernel(AdjLaunch3 a) {
     R lg[Q3];
     const R* xt = (const R*)a.xTab + 4 * x;
     R dut = R(0);
-    collide_adjoint3<R>(g, lp, xt[0], xt[1], xt[2], (R)__ldg(&a.uDev[adj_step(a)]), lg, dut);
+    // block-uniform: tiles that end before the absorbing layer take the code without it
+    if ((int)((blockIdx.x + 1) * blockDim.x) > a.absorbX0)
+      collide_adjoint3<R, true>(g, lp, xt[0], xt[1], xt[2], (R)__ldg(&a.uDev[adj_step(a)]), lg, dut);
+    else
+      collide_adjoint3<R, false>(g, lp, xt[0], xt[1], xt[2], (R)__ldg(&a.uDev[adj_step(a)]), lg, dut);
     du = (double)dut;
 #pragma unroll
     for (int i = 0; i < Q3; i++) lamOut[i * N + idx - (int)off3(i, W, H)] = lg[i];
@@ -728,6 +738,7 @@ AdjLaunch3 adj_args(Cells3D* h, Adjoint3D* A) {
   a.H = h->H;
   a.D = h->D;
   a.tileX = A->tileX;
+  a.absorbX0 = h->absorbX0;
   a.nCellBlocks = A->nBlocks;
   a.slowCells = A->slowCells;
   a.nSlow = A->nSlow;
@@ -897,7 +908,9 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
   A->endState = dev.alloc(sizeof(DevState3), "adjoint end state");
   A->lam[0] = dev.alloc(fBytes, "adjoint state");
   A->lam[1] = dev.alloc(fBytes, "adjoint state");
-  A->tileX = h->W >= 128 ? 128 : (h->W >= 64 ? 64 : 32);
+  // 32-cell x tiles: each warp still reads 128-byte rows, and the tiles before the absorbing layer
+  // take the collision code without it
+  A->tileX = 32;
   const int tileY = kAdjThreads / A->tileX;
   A->nBlocks = ((h->W + A->tileX - 1) / A->tileX) * ((h->H + tileY - 1) / tileY) * h->D;
   A->nParts = A->nBlocks + (A->nSlow + kSlowCells - 1) / kSlowCells;

@@ -129,6 +129,7 @@ struct AdjLaunch3 {
   long long N;
   int W, H, D;
   int tileX;             // cell kernel block: tileX x (kAdjThreads / tileX) cells of x-rows
+  int absorbX0;          // first x of the absorbing layer (W when there is none)
   int nCellBlocks;       // blocks of the cell kernel
   const int* slowCells;  // the flagged fluid cells, in index order
   int nSlow;

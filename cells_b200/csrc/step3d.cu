@@ -360,8 +360,46 @@ __host__ __device__ __forceinline__ int shell_rows3(int H, int D) {
   return nz * H + ny * inD;
 }
 
+// Whether direction i enters a face row's cells from outside the grid: SIDE 0 / 1 are the rows
+// y = 1 .. H-2 of the z = 0 / z = D-1 planes, 2 / 3 the y = 0 / y = H-1 rows of the planes between.
+template <int SIDE>
+__host__ __device__ __forceinline__ constexpr bool face_out3(int i) {
+  return SIDE == 0 ? cz3(i) == 1 : (SIDE == 1 ? cz3(i) == -1 : (SIDE == 2 ? cy3(i) == 1 : cy3(i) == -1));
+}
+
+// A cell of a face row with one outside side (pullSlow3, step3d.ts:119-168, for a cell without solid
+// neighbours): every direction's rule is fixed at compile time -- a plain pull, the slip face's
+// specular reflection from the same row or plane, or at the outlet column the zero-gradient copy
+// from x = W-2 -- and the pulls go out before the body-row test. x >= 1 (the caller handles the
+// inlet), so every source is inside the grid.
+template <class C, bool SMAG, int SIDE>
+__device__ __forceinline__ void face_row_cell3(const StepArgs3<C>& a, int x, int row, int idx) {
+  using R = typename C::R;
+  const int W = a.W, WH = a.W * a.H;
+  const bool outlet = x == W - 1;
+  R f[Q3];
+  f[0] = C::raw(a.src + idx);
+#pragma unroll
+  for (int i = 1; i < Q3; i++) {
+    int pop = i, cell;
+    if (cx3(i) == -1 && outlet) {
+      cell = (W - 2) + W * row;  // outlet: zero-gradient copy (the x rule comes first)
+    } else if (face_out3<SIDE>(i)) {
+      pop = SIDE < 2 ? mirror_z3(i) : mirror_y3(i);  // slip: specular reflection, own plane / row
+      cell = SIDE < 2 ? idx - (cx3(i) + cy3(i) * W) : idx - (cx3(i) + cz3(i) * WH);
+    } else {
+      cell = idx - (cx3(i) + cy3(i) * W + cz3(i) * WH);
+    }
+    f[i] = C::raw(a.src + (long long)pop * a.N + cell);
+  }
+  if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
+  collide_store<C, SMAG>(a, f, x, idx, outlet);
+}
+
 // A face cell: pullSlow3 (step3d.ts:119-168) for a cell without solid neighbours, every mirrored
-// source being fluid; the inlet cell stores the inflow equilibrium.
+// source being fluid; the inlet cell stores the inflow equilibrium. Rows with one outside side take
+// face_row_cell3; the y = 0 and y = H-1 rows of the z planes (edges) and grids thinner than three
+// cells take the general rules.
 template <class C, bool SMAG>
 __device__ __forceinline__ void shell_role(const StepArgs3<C>& a, int b, int tid) {
   using R = typename C::R;
@@ -373,28 +411,38 @@ __device__ __forceinline__ void shell_role(const StepArgs3<C>& a, int b, int tid
   const int x = (int)(((unsigned)b - rowK * bpr) * kStepThreads) + tid;
   if (x >= W) return;
   const unsigned rowsZ = (D >= 2 ? 2u : 1u) * (unsigned)H;
-  int y, z;
+  int y, z, side;  // side: 0..3 as in face_out3, 4 the general rules (block-uniform)
   if (rowK < rowsZ) {
     const unsigned plane = rowK / (unsigned)H;
     y = (int)(rowK - plane * (unsigned)H);
     z = plane == 0 ? 0 : D - 1;
+    side = (D >= 2 && y >= 1 && y <= H - 2) ? (plane == 0 ? 0 : 1) : 4;
   } else {
     const unsigned inD = (unsigned)(D - 2);
     const unsigned k = rowK - rowsZ;
-    const unsigned side = k / inD;
-    y = side == 0 ? 0 : H - 1;
-    z = 1 + (int)(k - side * inD);
+    const unsigned sideY = k / inD;
+    y = sideY == 0 ? 0 : H - 1;
+    z = 1 + (int)(k - sideY * inD);
+    side = H >= 2 ? (sideY == 0 ? 2 : 3) : 4;
   }
   const int row = y + H * z;
   const int idx = x + W * row;
-  if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
   if (x == 0) {
+    if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
     // inlet: equilibrium at the inflow speed, no collision (step3d.ts:190-193)
     const double* eq = a.st->inletEq[a.par];
 #pragma unroll
     for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw((R)eq[i]);
     return;
   }
+  switch (side) {
+    case 0: face_row_cell3<C, SMAG, 0>(a, x, row, idx); return;
+    case 1: face_row_cell3<C, SMAG, 1>(a, x, row, idx); return;
+    case 2: face_row_cell3<C, SMAG, 2>(a, x, row, idx); return;
+    case 3: face_row_cell3<C, SMAG, 3>(a, x, row, idx); return;
+    default: break;
+  }
+  if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
   const bool outlet = x == W - 1;
   const int WH = W * H;
   R f[Q3];

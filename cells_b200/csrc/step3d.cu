@@ -339,8 +339,7 @@ __device__ __forceinline__ double ramp_speed(int kind, double target, double ram
 //
 // Blocks of 128 threads take one of three roles by block index (computed on the host):
 //   [0, shellBlocks)                      the face cells: z = 0 and z = D-1 planes, y = 0 and y = H-1
-//                                         rows of the planes between, one cell per thread, each block
-//                                         128 cells of one face row;
+//                                         rows of the planes between, one cell per thread, x fastest;
 //   [shellBlocks, + bodyBlocks)           32 body cells per block, their 19 links resolved in parallel;
 //   [shellBlocks + bodyBlocks, + tiles)   the rows y = 1 .. H-2 of planes z = 1 .. D-2 in tiles of
 //                                         tileTY rows of tileTX cells (two cells per thread for
@@ -352,12 +351,12 @@ __device__ __forceinline__ double ramp_speed(int kind, double target, double ram
 
 constexpr int kStepThreads = 128;
 
-// Rows of W cells on the faces: the H rows of each of the z = 0 and z = D-1 planes, then the y = 0
-// and y = H-1 rows of the planes between. One face row takes ceil(W / kStepThreads) blocks.
-__host__ __device__ __forceinline__ int shell_rows3(int H, int D) {
-  const int nz = D >= 2 ? 2 : 1, ny = H >= 2 ? 2 : 1;
-  const int inD = D > 2 ? D - 2 : 0;
-  return nz * H + ny * inD;
+// Number of cells on the faces: the z = 0 and z = D-1 planes and the y = 0 and y = H-1 rows of the
+// planes between.
+__host__ __device__ __forceinline__ long long shell_cells3(int W, int H, int D) {
+  const long long nz = D >= 2 ? 2 : 1, ny = H >= 2 ? 2 : 1;
+  const long long inD = D > 2 ? D - 2 : 0;
+  return nz * W * H + ny * W * inD;
 }
 
 // Whether direction i enters a face row's cells from outside the grid: SIDE 0 / 1 are the rows
@@ -397,54 +396,61 @@ __device__ __forceinline__ void face_row_cell3(const StepArgs3<C>& a, int x, int
 }
 
 // A face cell: pullSlow3 (step3d.ts:119-168) for a cell without solid neighbours, every mirrored
-// source being fluid; the inlet cell stores the inflow equilibrium. Rows with one outside side take
-// face_row_cell3; the y = 0 and y = H-1 rows of the z planes (edges) and grids thinner than three
-// cells take the general rules.
+// source being fluid; the inlet cell stores the inflow equilibrium. With 16-bit storage, cells of
+// rows with one outside side take face_row_cell3 (its per-side code measured faster in the
+// issue-bound 16-bit kernels and slower in the memory-bound f32 / f64 ones, where the general
+// rules below stay).
 template <class C, bool SMAG>
 __device__ __forceinline__ void shell_role(const StepArgs3<C>& a, int b, int tid) {
   using R = typename C::R;
   const int W = a.W, H = a.H, D = a.D;
-  // block b: face row b / bpr, cells from (b % bpr) * kStepThreads; 32-bit arithmetic throughout
-  // (N < 2^31), one unsigned division by the row count and one by H per thread
-  const unsigned bpr = ((unsigned)W + kStepThreads - 1) / kStepThreads;
-  const unsigned rowK = (unsigned)b / bpr;
-  const int x = (int)(((unsigned)b - rowK * bpr) * kStepThreads) + tid;
-  if (x >= W) return;
-  const unsigned rowsZ = (D >= 2 ? 2u : 1u) * (unsigned)H;
-  int y, z, side;  // side: 0..3 as in face_out3, 4 the general rules (block-uniform)
-  if (rowK < rowsZ) {
-    const unsigned plane = rowK / (unsigned)H;
-    y = (int)(rowK - plane * (unsigned)H);
+  long long t = (long long)b * kStepThreads + tid;
+  int x, y, z;
+  bool onZ = false;  // a cell of the z = 0 or z = D-1 plane
+  const long long nzp = D >= 2 ? 2 : 1, nyr = H >= 2 ? 2 : 1;
+  const long long inD = D > 2 ? D - 2 : 0;
+  const long long cz = nzp * W * H, cy = nyr * W * inD;
+  if (t < cz) {
+    const long long plane = t / ((long long)W * H);
+    const long long r = t - plane * W * H;
     z = plane == 0 ? 0 : D - 1;
-    side = (D >= 2 && y >= 1 && y <= H - 2) ? (plane == 0 ? 0 : 1) : 4;
+    y = (int)(r / W);
+    x = (int)(r - (long long)y * W);
+    onZ = true;
+  } else if ((t -= cz) < cy) {
+    const long long side = t / (W * inD);
+    const long long r = t - side * W * inD;
+    y = side == 0 ? 0 : H - 1;
+    z = 1 + (int)(r / W);
+    x = (int)(r - (long long)(z - 1) * W);
   } else {
-    const unsigned inD = (unsigned)(D - 2);
-    const unsigned k = rowK - rowsZ;
-    const unsigned sideY = k / inD;
-    y = sideY == 0 ? 0 : H - 1;
-    z = 1 + (int)(k - sideY * inD);
-    side = H >= 2 ? (sideY == 0 ? 2 : 3) : 4;
+    return;
   }
   const int row = y + H * z;
   const int idx = x + W * row;
+  if constexpr (sizeof(typename C::S) == 2) {
+    // side as in face_out3 for rows with one outside side (edge rows and thin grids take the rules below)
+    const int side = onZ ? ((D >= 2 && y >= 1 && y <= H - 2) ? (z == 0 ? 0 : 1) : 4) : (H >= 2 ? (y == 0 ? 2 : 3) : 4);
+    if (x != 0 && side < 4) {
+      switch (side) {
+        case 0: face_row_cell3<C, SMAG, 0>(a, x, row, idx); return;
+        case 1: face_row_cell3<C, SMAG, 1>(a, x, row, idx); return;
+        case 2: face_row_cell3<C, SMAG, 2>(a, x, row, idx); return;
+        default: face_row_cell3<C, SMAG, 3>(a, x, row, idx); return;
+      }
+    }
+  }
+  if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
   if (x == 0) {
-    if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
     // inlet: equilibrium at the inflow speed, no collision (step3d.ts:190-193)
     const double* eq = a.st->inletEq[a.par];
 #pragma unroll
     for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw((R)eq[i]);
     return;
   }
-  switch (side) {
-    case 0: face_row_cell3<C, SMAG, 0>(a, x, row, idx); return;
-    case 1: face_row_cell3<C, SMAG, 1>(a, x, row, idx); return;
-    case 2: face_row_cell3<C, SMAG, 2>(a, x, row, idx); return;
-    case 3: face_row_cell3<C, SMAG, 3>(a, x, row, idx); return;
-    default: break;
-  }
-  if (a.rowBody[row] && __ldg(a.flags + idx) != 0u) return;
   const bool outlet = x == W - 1;
-  const int WH = W * H;
+  const long long N = a.N;
+  const long long WH = (long long)W * H;
   R f[Q3];
   f[0] = C::raw(a.src + idx);
 #pragma unroll
@@ -454,11 +460,11 @@ __device__ __forceinline__ void shell_role(const StepArgs3<C>& a, int b, int tid
     const bool outY = sy < 0 || sy >= H;
     const bool outZ = sz < 0 || sz >= D;
     int pop = i;
-    int cell;
+    long long cell;
     if (!(outX || outY || outZ)) {
-      cell = idx - (cx3(i) + cy3(i) * W + cz3(i) * WH);
+      cell = idx - (cx3(i) + cy3(i) * (long long)W + cz3(i) * WH);
     } else if (outX && outlet) {
-      cell = (W - 2) + W * row;  // outlet: zero-gradient copy
+      cell = (long long)(W - 2) + (long long)W * row;  // outlet: zero-gradient copy
     } else if (outY && outZ) {
       pop = opp3(i);  // edge: the double mirror equals bounce-back
       cell = idx;
@@ -466,12 +472,12 @@ __device__ __forceinline__ void shell_role(const StepArgs3<C>& a, int b, int tid
       pop = outY ? mirror_y3(i) : mirror_z3(i);  // slip: specular reflection
       const int ry = outY ? y : sy;
       const int rz = outY ? sz : z;
-      cell = sx + W * (ry + H * rz);
+      cell = (long long)sx + (long long)W * (ry + (long long)H * rz);
     } else {
       pop = opp3(i);
       cell = idx;
     }
-    f[i] = C::raw(a.src + (long long)pop * a.N + cell);
+    f[i] = C::raw(a.src + (long long)pop * N + cell);
   }
   collide_store<C, SMAG>(a, f, x, idx, outlet);
 }
@@ -809,7 +815,8 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   a.smagC2 = (R)L.smagC2;
   a.absorbX0 = L.absorbX0;
   // work split
-  a.shellBlocks = shell_rows3(L.H, L.D) * ((L.W + kStepThreads - 1) / kStepThreads);
+  const long long nShell = shell_cells3(L.W, L.H, L.D);
+  a.shellBlocks = (int)((nShell + kStepThreads - 1) / kStepThreads);
   // the body role runs when there are body cells, and on sampled steps even without them (a
   // sample of zero force is still written to the ring, as the reference's reduce pass does)
   a.bodyBlocks = (L.nBody > 0 || L.sample) ? body_blocks3(L.nBody) : 0;

@@ -5,8 +5,12 @@
 
 namespace cells {
 
+// Rows of cells each thread of the step kernel updates: a block of tileX x tileY threads covers a
+// tile of tileX x (kRows2 tileY) cells, its threads taking rows y and y + tileY.
+constexpr int kRows2 = 2;
+
 // One step (or, persistent, nSteps steps) of every tunnel of a batch. A tile is one block's cells:
-// tileX x tileY cells of one tunnel; the tiles of all tunnels are numbered consecutively.
+// tileX x (kRows2 tileY) cells of one tunnel; the tiles of all tunnels are numbered consecutively.
 struct Step2Launch {
   const Tunnel2* tunnels;            // device array, one per tunnel
   const unsigned short* tileTunnel;  // device array: the tunnel of each tile

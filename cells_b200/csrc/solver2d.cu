@@ -167,7 +167,7 @@ void Cells2DBatch::set_layout(int tx, int ty, int pers) {
   for (size_t k = 0; k < t.size(); k++) {
     Tunnel2Host& T = t[k];
     T.tilesX = (T.W + tx - 1) / tx;
-    T.nTiles = T.tilesX * ((T.H + ty - 1) / ty);
+    T.nTiles = T.tilesX * ((T.H + kRows2 * ty - 1) / (kRows2 * ty));
     if (T.nTiles > T.partialsCap) throw Error(CELLS_E_INVALID, "tile shape needs more force partials than allocated");
     T.firstTile = first;
     first += T.nTiles;

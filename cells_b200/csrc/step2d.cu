@@ -166,12 +166,26 @@ struct Hot2 {
   typename C::R smagC2;
 };
 
-// main, src/shaders/step.ts:177-227, for the cell (x, y) of tunnel T. Returns whether the cell has
-// a force slot (its force is then in force[0..1]). The x-dependent rates come from the tunnel's x
-// table; the exact build evaluates every other expression in the reference's order.
+// The loads of the cell (x, y): its flag word and the fast path's nine pulls, issued together (one
+// memory round trip per cell, not two); a flagged cell replaces the pulls in cell2. Every address is
+// inside the allocation: the largest, direction 8 on the top row, is at most W - 1 elements past the
+// nine arrays, which the host pads.
+template <class C>
+__device__ __forceinline__ uint32_t load2(const Hot2<C>& h, int x, int y, typename C::R (&f)[Q2]) {
+  using R = typename C::R;
+  const int idx = y * h.W + x;
+#pragma unroll
+  for (int i = 0; i < Q2; i++) f[i] = (R)C::ld(h.src + (i * h.N + idx - cy2(i) * h.W - cx2(i)));
+  return __ldg(&h.flags[idx]);
+}
+
+// main, src/shaders/step.ts:177-227, for the cell (x, y) of tunnel T, whose loads load2 made.
+// Returns whether the cell has a force slot (its force is then in force[0..1]). The x-dependent
+// rates come from the tunnel's x table; the exact build evaluates every other expression in the
+// reference's order.
 template <class C>
 __device__ __forceinline__ bool cell2(const Tunnel2& T, const Hot2<C>& h, typename C::R uIn, int x, int y,
-                                      typename C::R force[2]) {
+                                      uint32_t fl, typename C::R (&f)[Q2], typename C::R force[2]) {
   using R = typename C::R;
   using S = typename C::S;
   const int W = h.W;
@@ -179,14 +193,6 @@ __device__ __forceinline__ bool cell2(const Tunnel2& T, const Hot2<C>& h, typena
   const S* __restrict__ src = h.src;
   S* __restrict__ dst = h.dst;
   const int idx = y * W + x;
-  const uint32_t fl = __ldg(&h.flags[idx]);
-  // the fast path's nine pulls go out together with the flag load (one memory round trip per cell,
-  // not two); a flagged cell replaces them below. Every address is inside the allocation: the
-  // largest, direction 8 on the top row, is at most W - 1 elements past the nine arrays, which the
-  // host pads.
-  R f[Q2];
-#pragma unroll
-  for (int i = 0; i < Q2; i++) f[i] = (R)C::ld(src + (i * N + idx - cy2(i) * W - cx2(i)));
   bool slot = false;
   if (fl != 0u) {
     if (fl & FLAG2_SOLID) return false;
@@ -329,7 +335,7 @@ __device__ __forceinline__ void tile2(const Tunnel2* __restrict__ tunnels, int t
   const int tyi = lb / tilesX;
   const int txi = lb - tyi * tilesX;
   const int x = txi * blockDim.x + threadIdx.x;
-  const int y = tyi * blockDim.y + threadIdx.y;
+  const int y = tyi * (kRows2 * blockDim.y) + threadIdx.y;  // this thread's rows: y + k blockDim.y
   DevState2* st = T.st;
   const unsigned step = __ldcg(&st->step[par]);
   const double uInD = __ldcg(&st->uIn[par]);
@@ -341,8 +347,10 @@ __device__ __forceinline__ void tile2(const Tunnel2* __restrict__ tunnels, int t
     st->uIn[par ^ 1] = T.rampKind != 0 ? ramp_speed2(T.rampKind, T.rampTarget, T.rampSteps, T.rampEvery, step + 1u)
                                        : uInD;
   }
-  R force[2] = {R(0), R(0)};
-  bool slot = false;
+  // each cell's force stays in its own accumulator and is widened to f64 before the two are added,
+  // as every cell's force enters the f64 tile sum on its own
+  R force[2] = {R(0), R(0)}, force1[2] = {R(0), R(0)};
+  bool slot = false, slot1 = false;
   if (x < T.W && y < T.H) {
     Hot2<C> h;
     h.W = T.W;
@@ -354,12 +362,24 @@ __device__ __forceinline__ void tile2(const Tunnel2* __restrict__ tunnels, int t
     h.xtab = (const typename XTab2<R>::T*)T.xtab;
     h.forcing = T.forcing;
     h.smagC2 = prm<R>(T, P2_SMAGC2);
-    slot = cell2<C>(T, h, (R)uInD, x, y, force);
+    // both rows' loads go out before either cell computes
+    const int y1 = y + blockDim.y;
+    const bool second = y1 < h.H;
+    R f0[Q2], f1[Q2];
+    const uint32_t fl0 = load2<C>(h, x, y, f0);
+    uint32_t fl1 = 0u;
+    if (second) fl1 = load2<C>(h, x, y1, f1);
+    slot = cell2<C>(T, h, (R)uInD, x, y, fl0, f0, force);
+    if (second) slot1 = cell2<C>(T, h, (R)uInD, x, y1, fl1, f1, force1);
   }
   if (!sample) return;
   // f64 sum of the tile's forces: warp shuffles, then warps in order
-  if (__syncthreads_or(slot ? 1 : 0)) {
+  if (__syncthreads_or((slot || slot1) ? 1 : 0)) {
     double sx = slot ? (double)force[0] : 0.0, sy = slot ? (double)force[1] : 0.0;
+    if (slot1) {
+      sx += (double)force1[0];
+      sy += (double)force1[1];
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       sx += __shfl_down_sync(0xffffffffu, sx, o);

@@ -5,17 +5,15 @@
 
 namespace cells {
 
-// Rows of cells each thread of the step kernel updates: a block of tileX x tileY threads covers a
-// tile of tileX x (kRows2 tileY) cells, its threads taking rows y and y + tileY.
-constexpr int kRows2 = 2;
-
 // One step (or, persistent, nSteps steps) of every tunnel of a batch. A tile is one block's cells:
-// tileX x (kRows2 tileY) cells of one tunnel; the tiles of all tunnels are numbered consecutively.
+// tileX x (rows tileY) cells of one tunnel, each thread taking rows y and, with rows = 2, y + tileY;
+// the tiles of all tunnels are numbered consecutively.
 struct Step2Launch {
   const Tunnel2* tunnels;            // device array, one per tunnel
   const unsigned short* tileTunnel;  // device array: the tunnel of each tile
   int nTiles;                        // tiles of all tunnels
-  int tileX, tileY;                  // block shape (threads = cells of a tile)
+  int tileX, tileY;                  // block shape
+  int rows;                          // cell rows per thread: 1 or 2
   int par;                           // parity of the first step
   int allowSample;                   // 0: no force sampling (autotuner trials)
   int nSteps;                        // persistent launch: steps per launch

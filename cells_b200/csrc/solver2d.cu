@@ -99,6 +99,7 @@ struct Cells2DBatch : HandleBase {
 
   // launch layout
   int tileX = 32, tileY = 4;
+  int rows = 1;  // cell rows per thread of the step kernel
   int persistent = 0;
   int persistentBlocks = 0;
   int nTiles = 0;
@@ -162,12 +163,17 @@ void Cells2DBatch::set_layout(int tx, int ty, int pers) {
   tileX = tx;
   tileY = ty;
   persistent = pers;
+  // two cell rows per thread (both rows' loads in flight together) when the batch is large enough
+  // to fill the GPU with the halved block count; small grids keep one row and twice the blocks
+  long long tiles1 = 0;
+  for (const Tunnel2Host& T : t) tiles1 += (long long)((T.W + tx - 1) / tx) * ((T.H + ty - 1) / ty);
+  rows = tiles1 >= 4096 ? 2 : 1;
   std::vector<unsigned short> map;
   int first = 0;
   for (size_t k = 0; k < t.size(); k++) {
     Tunnel2Host& T = t[k];
     T.tilesX = (T.W + tx - 1) / tx;
-    T.nTiles = T.tilesX * ((T.H + kRows2 * ty - 1) / (kRows2 * ty));
+    T.nTiles = T.tilesX * ((T.H + rows * ty - 1) / (rows * ty));
     if (T.nTiles > T.partialsCap) throw Error(CELLS_E_INVALID, "tile shape needs more force partials than allocated");
     T.firstTile = first;
     first += T.nTiles;
@@ -308,6 +314,7 @@ void Cells2DBatch::launch_raw(int64_t n, int par, int allowSample) {
   a.nTiles = nTiles;
   a.tileX = tileX;
   a.tileY = tileY;
+  a.rows = rows;
   a.allowSample = allowSample;
   a.barrier = dBarrier;
   a.error = dError;
@@ -354,6 +361,7 @@ void Cells2DBatch::build_graph(int allowSample, int par) {
   a.nTiles = nTiles;
   a.tileX = tileX;
   a.tileY = tileY;
+  a.rows = rows;
   a.allowSample = allowSample;
   a.nSteps = 1;
   a.gridBlocks = 0;

@@ -323,7 +323,7 @@ __device__ __forceinline__ double ramp_speed2(int kind, double target, double ra
 }
 
 // One tile (lb-th of its tunnel t) of the step of parity par.
-template <class C>
+template <class C, int ROWS>
 __device__ __forceinline__ void tile2(const Tunnel2* __restrict__ tunnels, int t, int lb, int par, int allowSample) {
   using R = typename C::R;
   const Tunnel2& T = tunnels[t];
@@ -335,7 +335,7 @@ __device__ __forceinline__ void tile2(const Tunnel2* __restrict__ tunnels, int t
   const int tyi = lb / tilesX;
   const int txi = lb - tyi * tilesX;
   const int x = txi * blockDim.x + threadIdx.x;
-  const int y = tyi * (kRows2 * blockDim.y) + threadIdx.y;  // this thread's rows: y + k blockDim.y
+  const int y = tyi * (ROWS * blockDim.y) + threadIdx.y;  // this thread's rows: y (+ blockDim.y)
   DevState2* st = T.st;
   const unsigned step = __ldcg(&st->step[par]);
   const double uInD = __ldcg(&st->uIn[par]);
@@ -362,15 +362,20 @@ __device__ __forceinline__ void tile2(const Tunnel2* __restrict__ tunnels, int t
     h.xtab = (const typename XTab2<R>::T*)T.xtab;
     h.forcing = T.forcing;
     h.smagC2 = prm<R>(T, P2_SMAGC2);
-    // both rows' loads go out before either cell computes
-    const int y1 = y + blockDim.y;
-    const bool second = y1 < h.H;
-    R f0[Q2], f1[Q2];
+    R f0[Q2];
     const uint32_t fl0 = load2<C>(h, x, y, f0);
-    uint32_t fl1 = 0u;
-    if (second) fl1 = load2<C>(h, x, y1, f1);
-    slot = cell2<C>(T, h, (R)uInD, x, y, fl0, f0, force);
-    if (second) slot1 = cell2<C>(T, h, (R)uInD, x, y1, fl1, f1, force1);
+    if constexpr (ROWS == 2) {
+      // both rows' loads go out before either cell computes
+      const int y1 = y + blockDim.y;
+      const bool second = y1 < h.H;
+      R f1[Q2];
+      uint32_t fl1 = 0u;
+      if (second) fl1 = load2<C>(h, x, y1, f1);
+      slot = cell2<C>(T, h, (R)uInD, x, y, fl0, f0, force);
+      if (second) slot1 = cell2<C>(T, h, (R)uInD, x, y1, fl1, f1, force1);
+    } else {
+      slot = cell2<C>(T, h, (R)uInD, x, y, fl0, f0, force);
+    }
   }
   if (!sample) return;
   // f64 sum of the tile's forces: warp shuffles, then warps in order
@@ -443,13 +448,13 @@ constexpr int min_blocks2() {
   return sizeof(typename C::R) == 4 ? 4 : 1;
 }
 
-template <class C>
+template <class C, int ROWS>
 __global__ void __launch_bounds__(256, min_blocks2<C>()) step2d_kernel(const Tunnel2* __restrict__ tunnels,
                                                      const unsigned short* __restrict__ tileTunnel, int par,
                                                      int allowSample) {
   const int b = blockIdx.x;
   const int t = __ldg(&tileTunnel[b]);
-  tile2<C>(tunnels, t, b - __ldg(&tunnels[t].firstTile), par, allowSample);
+  tile2<C, ROWS>(tunnels, t, b - __ldg(&tunnels[t].firstTile), par, allowSample);
 }
 
 // Grid-wide barrier of the persistent kernel: arrivals count up a counter that the host zeroes
@@ -482,7 +487,7 @@ __device__ __forceinline__ bool grid_barrier2(unsigned* counter, unsigned target
 
 // nSteps steps of every tunnel in one launch: each resident block walks the tiles with a grid
 // stride, then all blocks meet at the barrier before the next step.
-template <class C>
+template <class C, int ROWS>
 __global__ void __launch_bounds__(256, min_blocks2<C>()) step2d_persistent_kernel(const Tunnel2* __restrict__ tunnels,
                                                                 const unsigned short* __restrict__ tileTunnel,
                                                                 int nTiles, int par, int nSteps, int allowSample,
@@ -490,7 +495,7 @@ __global__ void __launch_bounds__(256, min_blocks2<C>()) step2d_persistent_kerne
   for (int s = 0; s < nSteps; s++) {
     for (int b = blockIdx.x; b < nTiles; b += gridDim.x) {
       const int t = __ldg(&tileTunnel[b]);
-      tile2<C>(tunnels, t, b - __ldg(&tunnels[t].firstTile), par, allowSample);
+      tile2<C, ROWS>(tunnels, t, b - __ldg(&tunnels[t].firstTile), par, allowSample);
       __syncthreads();
     }
     par ^= 1;
@@ -502,7 +507,10 @@ template <class C>
 static cudaError_t launch_step2_t(const Step2Launch& a, cudaStream_t s) {
   if (a.nTiles <= 0) return cudaSuccess;
   dim3 block(a.tileX, a.tileY);
-  step2d_kernel<C><<<a.nTiles, block, 0, s>>>(a.tunnels, a.tileTunnel, a.par, a.allowSample);
+  if (a.rows == 2)
+    step2d_kernel<C, 2><<<a.nTiles, block, 0, s>>>(a.tunnels, a.tileTunnel, a.par, a.allowSample);
+  else
+    step2d_kernel<C, 1><<<a.nTiles, block, 0, s>>>(a.tunnels, a.tileTunnel, a.par, a.allowSample);
   return cudaGetLastError();
 }
 
@@ -518,7 +526,8 @@ static cudaError_t launch_step2_persistent_t(const Step2Launch& a, cudaStream_t 
   void* args[] = {&tunnels, &tileTunnel, &nTiles, &par, &nSteps, &allowSample, &barrier, &error};
   cudaError_t e = cudaMemsetAsync(barrier, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
-  return cudaLaunchCooperativeKernel((const void*)step2d_persistent_kernel<C>, dim3(a.gridBlocks), block, args, 0, s);
+  const void* fn = a.rows == 2 ? (const void*)step2d_persistent_kernel<C, 2> : (const void*)step2d_persistent_kernel<C, 1>;
+  return cudaLaunchCooperativeKernel(fn, dim3(a.gridBlocks), block, args, 0, s);
 }
 
 template <class C>
@@ -526,8 +535,12 @@ static int persistent_blocks2_t(int threads) {
   int dev = 0, sms = 0, perSm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, step2d_persistent_kernel<C>, threads, 0) != cudaSuccess)
+  // resident blocks of either rows variant (the smaller, so that both launch cooperatively)
+  int perSm2 = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, step2d_persistent_kernel<C, 1>, threads, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm2, step2d_persistent_kernel<C, 2>, threads, 0) != cudaSuccess)
     return 0;
+  if (perSm2 < perSm) perSm = perSm2;
   return perSm * sms;
 }
 

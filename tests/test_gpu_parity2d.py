@@ -238,6 +238,38 @@ def test_batch_matches_oracle_per_tunnel(launch):
     b.destroy()
 
 
+def test_batch_two_rows_per_thread_matches_oracle():
+    """A batch of 4,096 tiles or more takes the kernel with two cell rows per thread; 2 tunnels of
+    1000 x 253 (32 x 64 tiles of 32 x 4 threads each) reach it, with an odd height (the last row pair
+    of a column has one row) and a width that is not a multiple of the tile."""
+    W, H = 1000, 253
+    cfgs = [dict(width=W, height=H, left=XMode.Open, right=XMode.Open, bottom=YMode.Slip, top=YMode.Slip,
+                 tau=0.56, uIn=0.08, smagorinsky=0.1, spongeFraction=0.15, absorb=0.02, forceEvery=1),
+            dict(width=W, height=H, left=XMode.Periodic, right=XMode.Periodic, bottom=YMode.NoSlip,
+                 top=YMode.NoSlip, tau=0.7, bodyForce=(1e-6, 0.0), forceEvery=3)]
+    b = Batch2D([dict(c, exactArithmetic=True) for c in cfgs])
+    b.setLaunch(32, 4, False)
+    oracles = []
+    for t, c in zip(b.tunnels, cfgs):
+        sdf = circle_sdf(W, H, W / 4, H / 2 + 0.3, 12.0)
+        kw = {k: v for k, v in c.items() if k not in ("width", "height")}
+        o = OracleSolver2D(W, H, **kw)
+        t.setSdf(sdf)
+        o.setSdf(sdf)
+        m = perturbed_rest2(W, H, 1e-4)
+        t.initField(m)
+        o.initField(m)
+        oracles.append(o)
+    b.step(3)
+    b.step(100)  # one graph of 100 steps
+    for o in oracles:
+        o.encodeSteps(103)
+    for t, o in zip(b.tunnels, oracles):
+        assert_same(t.readPopulations(), o.populations(), True)
+        assert_forces(t.readForces(), o.readForces())
+    b.destroy()
+
+
 def test_autotune_keeps_state_and_results():
     cfgs = batch_configs()
     a = Batch2D([dict(c, exactArithmetic=True) for c in cfgs])

@@ -101,12 +101,14 @@ def test_sphere_fast_16bit_within_storage_rounding(precision, tol):
     s.destroy()
 
 
-def test_smagorinsky_fixed_lambda_cylinder_touching_slip_faces():
-    """A spanwise cylinder meets both z faces: the slip-face bounce-back with its force branch."""
+@pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16"])
+def test_smagorinsky_fixed_lambda_cylinder_touching_slip_faces(precision):
+    """A spanwise cylinder meets both z faces: the slip-face bounce-back with its force branch (the
+    16-bit kernels take the per-side face rows and the Smagorinsky pair collision)."""
     W, H, D = 20, 12, 10
     sdf = g.empty_sdf3(W, H, D)
     g.add_cylinder_z(sdf, W, H, D, 7, 6, 2.5)
-    s, o = pair(W, H, D, "fp32", True, sdf, smagorinsky=0.1, lambda_=3 / 16)
+    s, o = pair(W, H, D, precision, True, sdf, smagorinsky=0.1, lambda_=3 / 16)
     s.encodeSteps(20)
     o.encodeSteps(20)
     assert_same(s, o, True)
@@ -125,14 +127,15 @@ def test_odd_sizes_box_fp64():
     s.destroy()
 
 
-def test_body_touching_y_face_and_edges():
+@pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16"])
+def test_body_touching_y_face_and_edges(precision):
     """A sphere cut by the y = 0 face and a box through a z edge: mirrored sources on solids and
-    edge links."""
+    edge links (face cells of body rows go to the body role in every precision)."""
     W, H, D = 22, 10, 10
     sdf = g.empty_sdf3(W, H, D)
     g.add_sphere(sdf, W, H, D, 8, 0.5, 5, 3)
     g.add_box3(sdf, W, H, D, 14, 9, 9, 1.5, 1.5, 1.5)
-    s, o = pair(W, H, D, "fp32", True, sdf)
+    s, o = pair(W, H, D, precision, True, sdf)
     s.encodeSteps(12)
     o.encodeSteps(12)
     assert_same(s, o, True)

@@ -116,6 +116,20 @@ def test_smagorinsky_fixed_lambda_cylinder_touching_slip_faces(precision):
     s.destroy()
 
 
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+def test_odd_width_16bit_exact(precision):
+    """An odd width: 16-bit storage takes the one-cell-per-thread interior kernel (16-bit loads)
+    instead of x-pairs, with the per-side face rows."""
+    W, H, D = 23, 14, 10
+    s, o = pair(W, H, D, precision, True, sphere_sdf(W, H, D, 8, 7, 5, 3))
+    for n in (1, 20):
+        s.encodeSteps(n)
+        o.encodeSteps(n)
+        assert_same(s, o, True)
+    assert_forces(s.readForces(), o.readForces(), 1e-9)
+    s.destroy()
+
+
 def test_odd_sizes_box_fp64():
     W, H, D = 19, 7, 5
     sdf = g.empty_sdf3(W, H, D)

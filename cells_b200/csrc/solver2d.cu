@@ -1184,6 +1184,12 @@ int cells2d_batch_autotune(Cells2DBatch* b, int32_t trial_steps, Cells2DInfo* in
         if (pers && b->persistentBlocks <= 0) continue;
         b->dev.memset0(b->dError, sizeof(int));
         b->launch_raw(warm, par0, 0);
+        // a graph-replayed trial times the replay, not the capture: the layout change invalidated
+        // the step graphs, so they are rebuilt here, outside the timed region
+        if (!pers && b->useGraphs && trial_steps >= kGraphSteps2) {
+          b->build_graph(0, 0);
+          b->build_graph(0, 1);
+        }
         check_cuda(cudaEventRecord(b->dev.ev0, b->dev.stream), "cudaEventRecord");
         b->launch_raw(trial_steps, par0 ^ (warm & 1), 0);
         check_cuda(cudaEventRecord(b->dev.ev1, b->dev.stream), "cudaEventRecord");

@@ -517,9 +517,14 @@ static Cells2DBatch* create_batch(const Cells2DConfig* cfgs, int count) {
     b->massPartials = (double*)b->dev.alloc((size_t)b->nMassPartials * 8, "mass partials");
     b->massOut = (double*)b->dev.alloc(8, "mass result");
     b->dev.memset0(b->dError, 64);
+    // the initial launch shape: 32 x (workgroup_size / 32) threads when a size is given; by default
+    // 64 x 2, which the autotuner picked for a single 400 x 100 tunnel (cells2d_batch_autotune
+    // retunes a batch for its own sizes)
     const int wg = cfgs[0].workgroup_size;
-    const int ty = wg == 64 ? 2 : (wg == 256 ? 8 : 4);
-    b->set_layout(32, ty, 0);
+    if (wg == 0)
+      b->set_layout(64, 2, 0);
+    else
+      b->set_layout(32, wg == 64 ? 2 : (wg == 256 ? 8 : 4), 0);
     for (int k = 0; k < count; k++) {
       b->write_state(k, 1 | 2 | 4 | 8);
       b->rebuild_flags(k);

@@ -300,7 +300,7 @@ typedef struct {
   double body_force[2];       /* Guo body force (fx, fy) */
   double absorb;              /* peak rate of the absorbing layers */
   double inlet_layer_fraction;/* fraction of the length, from the inlet, with an absorbing layer */
-  int32_t workgroup_size;     /* threads per block: 64, 128 or 256; 0 = default (128) */
+  int32_t workgroup_size;     /* threads per block: 64, 128 or 256 (rows of 32); 0 = default (64 x 2) */
   int32_t force_every;        /* sample the obstacle force every n steps; 0 disables */
   int32_t device;             /* CUDA device ordinal, or CELLS_FAKE_DEVICE */
   int32_t fake_fail_alloc;    /* fake device only: the n-th allocation fails (0 = none) */

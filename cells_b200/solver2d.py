@@ -306,11 +306,16 @@ class Batch2D:
         check(lib().cells2d_batch_synchronize(self._h), self._h)
 
     def autotune(self, trialSteps: int = 100) -> dict:
+        """Times trialSteps steps of every launch shape (9 block shapes x per-step graph replay or the
+        persistent kernel) on a copy of the state, keeps the fastest and restores the state; returns
+        the chosen shape (tile_x, tile_y, persistent)."""
         i = _lib.Cells2DInfo()
         check(lib().cells2d_batch_autotune(self._h, trialSteps, C.byref(i)), self._h)
         return {k: getattr(i, k) for k, _ in i._fields_}
 
     def setLaunch(self, tileX: int, tileY: int, persistent: bool) -> None:
+        """Fixes the launch shape: tileX x tileY threads per block (64, 128 or 256); batches of 4,096
+        tiles or more give each thread two cell rows."""
         check(lib().cells2d_batch_set_launch(self._h, tileX, tileY, 1 if persistent else 0), self._h)
 
     def info(self) -> dict:

@@ -393,7 +393,8 @@ int cells2d_batch_synchronize(Cells2DBatch* b);
  * chosen shape to *info when info is not NULL. */
 int cells2d_batch_autotune(Cells2DBatch* b, int32_t trial_steps, Cells2DInfo* info);
 /* Fixes the launch shape by hand: tile_x * tile_y threads (64, 128 or 256, tile_x a multiple of 32),
- * persistent 0 or 1. */
+ * persistent 0 or 1. A block covers tile_x x tile_y cells, or tile_x x 2 tile_y (two rows per
+ * thread) when the batch has 4,096 tiles or more at one row per thread. */
 int cells2d_batch_set_launch(Cells2DBatch* b, int32_t tile_x, int32_t tile_y, int32_t persistent);
 int cells2d_batch_get_info(Cells2DBatch* b, Cells2DInfo* info);
 int cells2d_batch_timer_start(Cells2DBatch* b);

@@ -3,9 +3,9 @@
 * The 400x100 cylinder tunnel (D = 20 at (80, 50.5), Re 100, linear ramp to 0.1 over 3000 steps,
   20,000 steps): exact arithmetic reproduces the oracle's force trace and final field bit for bit;
   fast arithmetic keeps C_D, the C_L amplitude and St within 1% of the oracle's.
-* Validation cases of src/cases.ts with their acceptance ranges unchanged: plane Poiseuille,
-  Taylor-Green, periodic-seam invariance and the unconfined cylinder (St 0.165 +- 4%, mean C_D
-  1.345 +- 5%).
+* The eight validation cases of src/cases.ts with their acceptance ranges unchanged: plane
+  Poiseuille, Taylor-Green, periodic-seam invariance, Schafer-Turek 2D-1 and 2D-2, the unconfined
+  cylinder (St 0.165 +- 4%, mean C_D 1.345 +- 5%), the Ghia lid-driven cavity and NACA0012 at Re 500.
 """
 import math
 
@@ -57,7 +57,8 @@ def test_cylinder_tunnel_fast_within_one_percent(oracle_cylinder):
         assert abs(got[k] - ref[k]) <= 0.01 * abs(ref[k]), (k, got[k], ref[k])
 
 
-@pytest.mark.parametrize("key", ["poiseuille", "taylorGreen", "periodicSeam"])
+@pytest.mark.parametrize("key", ["poiseuille", "taylorGreen", "periodicSeam", "schaferTurek1", "schaferTurek2",
+                                 "cavity", "naca"])
 def test_reference_validation_case(key):
     r = cases2d.run_case(key)
     print(r["name"], [(m["name"], m["value"]) for m in r["metrics"]], f"{r['seconds']:.1f} s")

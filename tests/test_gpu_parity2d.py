@@ -270,7 +270,10 @@ def test_batch_two_rows_per_thread_matches_oracle():
     b.destroy()
 
 
-def test_autotune_keeps_state_and_results():
+@pytest.mark.parametrize("trial_steps", [40, 100])
+def test_autotune_keeps_state_and_results(trial_steps):
+    """Trials of 100 steps or more time graph replays (graphs rebuilt before the timed region), so
+    both trial kinds run; the state is restored and later steps match an untuned batch."""
     cfgs = batch_configs()
     a = Batch2D([dict(c, exactArithmetic=True) for c in cfgs])
     ref = Batch2D([dict(c, exactArithmetic=True) for c in cfgs])
@@ -280,7 +283,7 @@ def test_autotune_keeps_state_and_results():
             t.initField(perturbed_rest2(c["width"], c["height"], 1e-4))
         bb.step(11)
     before = [t.readPopulations() for t in a.tunnels]
-    info = a.autotune(40)
+    info = a.autotune(trial_steps)
     assert info["tile_x"] * info["tile_y"] in (64, 128, 256)
     for t, p in zip(a.tunnels, before):
         assert_same(t.readPopulations(), p, True)

@@ -272,3 +272,130 @@ def test_state_snapshot_resumes_bit_for_bit():
     assert t.step == s.step == 287
     s.destroy()
     t.destroy()
+
+
+# ---------------------------------------------------------------- grids wider than one x tile
+#
+# The interior kernel is chosen per block from the tile's x range: tiles that end before the first
+# absorbing column compile without the absorbing sources (ABS = false), tiles that do not hold the
+# outlet column without its rules (OUT = false). At W = 200 the FP32 / FP64 kernels take 7 tiles of
+# 32 cells (tiles 0-4 ABS = OUT = false, tile 5 ABS only, tile 6 both) and the 16-bit x-pair kernel
+# 4 tiles of 64 cells (tiles 0-1 neither, tile 2 ABS only, tile 3 both). With absorb = 0 every tile
+# has ABS = false and the last one OUT = true. The bodies sit in tiles of each kind, so body rows
+# (the flag test of the pair kernel) occur in each too.
+
+WIDE = (200, 12, 10)
+
+
+def wide_sdf():
+    W, H, D = WIDE
+    sdf = g.empty_sdf3(W, H, D)
+    g.add_sphere(sdf, W, H, D, 41, 6, 5, 3)      # FP32 tile 1, pair tile 0
+    g.add_sphere(sdf, W, H, D, 99.5, 5, 4, 2.5)  # FP32 tile 3, pair tile 1, across two x tiles
+    g.add_box3(sdf, W, H, D, 178, 7, 5, 2, 2, 2)  # FP32 tile 5, pair tile 2: inside the absorbing layer
+    return sdf
+
+
+@pytest.mark.parametrize("absorb", [0.02, 0.0])
+@pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16", "fp64"])
+def test_multi_tile_exact(precision, absorb):
+    W, H, D = WIDE
+    s, o = pair(W, H, D, precision, True, wide_sdf(), absorb=absorb)
+    info = s.info()
+    tile = 64 if precision in ("fp16", "bf16") else 32
+    assert info["block_x"] == tile, info  # tile width in cells
+    assert np.array_equal(s.readFlags(), o.flags)
+    for n in (1, 4, 20):
+        s.encodeSteps(n)
+        o.encodeSteps(n)
+        assert_same(s, o, True)
+    assert_forces(s.readForces(), o.readForces(), 1e-9)
+    s.destroy()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", 2e-6), ("fp16", 1e-4), ("bf16", 1e-3)])
+def test_multi_tile_fast(precision, tol):
+    W, H, D = WIDE
+    s, o = pair(W, H, D, precision, False, wide_sdf())
+    for n in (1, 29):
+        s.encodeSteps(n)
+        o.encodeSteps(n)
+        assert_same(s, o, False, tol)
+    assert_forces(s.readForces(), o.readForces(), 1e-5 if precision == "fp32" else 2e-2)
+    s.destroy()
+
+
+# ---------------------------------------------------------------- the 192x96x96 benchmark tunnel
+
+
+def config2_pair(exact, precision="fp32"):
+    """The benchmark's D3Q19 tunnel (192x96x96, sphere d = 16 at (48, 48, 48), Re 200, sponge over the
+    last 15% with absorb 0.02) on the GPU and on the oracle, started at the inflow speed 0.1 with
+    the seeded 1e-4 transverse perturbation."""
+    from cells_b200.units import derive_tau
+
+    W, H, D = 192, 96, 96
+    tau = derive_tau(200, 0.1, 16).tau
+    cfg = dict(tau=tau, uIn=0.1, spongeFraction=0.15, spongeTau=1.0, absorb=0.02, forceEvery=1)
+    s = Solver3D.create(W, H, D, precision=precision, exactArithmetic=exact, **cfg)
+    o = OracleSolver3D(W, H, D, precision, **cfg)
+    sdf = sphere_sdf(W, H, D, 48, 48, 48, 8)
+    m = perturbed_rest3(W, H, D, 1e-4, ux=0.1)
+    for x in (s, o):
+        x.setSdf(sdf)
+        x.initField(m)
+    return s, o
+
+
+def velocity_l2(a, b):
+    """Relative L2 norm of the velocity difference over the cells where b is fluid (rho != 0)."""
+    a = a.reshape(-1, 4).astype(np.float64)
+    b = b.reshape(-1, 4).astype(np.float64)
+    fl = b[:, 3] != 0
+    du = a[fl, :3] - b[fl, :3]
+    return float(np.sqrt(np.sum(du * du) / np.sum(b[fl, :3] ** 2)))
+
+
+def test_config2_exact_bit_for_bit():
+    """50 steps of the 192x96x96 tunnel: every population bit-identical to the oracle, so the tiles
+    of every interior variant at the benchmark's size (two 64-cell tiles without the absorbing layer
+    or the outlet, one with both), the face rows and the body are all checked."""
+    s, o = config2_pair(True)
+    s.encodeSteps(50)
+    o.encodeSteps(50)
+    assert_same(s, o, True)
+    assert_forces(s.readForces(), o.readForces(), 1e-9)
+    s.destroy()
+
+
+def test_config2_fast_against_oracle():
+    """200 steps of the 192x96x96 tunnel with the fast (FMA-contracted) kernel against the exact
+    oracle: populations within 2e-6, the velocity field's relative L2 difference <= 1e-4, every force
+    sample within 1e-5 relative."""
+    s, o = config2_pair(False)
+    s.encodeSteps(200)
+    o.encodeSteps(200)
+    assert_same(s, o, False, 2e-6)
+    assert_forces(s.readForces(), o.readForces(), 1e-5)
+    s.run(0)
+    o.run(0)
+    l2 = velocity_l2(s.readMacro(), o.readMacro())
+    print("velocity L2", l2)
+    assert l2 <= 1e-4
+    s.destroy()
+
+
+def test_config2_fp16_fast_against_oracle():
+    """The same tunnel with FP16 storage, 100 steps: populations within a few storage ulps (1e-4) of
+    the exact FP16 oracle, velocity L2 <= 1e-3, force samples within 1e-3 relative."""
+    s, o = config2_pair(False, "fp16")
+    s.encodeSteps(100)
+    o.encodeSteps(100)
+    assert_same(s, o, False, 1e-4)
+    assert_forces(s.readForces(), o.readForces(), 1e-3)
+    s.run(0)
+    o.run(0)
+    l2 = velocity_l2(s.readMacro(), o.readMacro())
+    print("velocity L2", l2)
+    assert l2 <= 1e-3
+    s.destroy()

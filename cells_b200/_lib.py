@@ -120,6 +120,7 @@ def lib() -> C.CDLL:
         "cells3d_read_forces_begin": (I, [P]),
         "cells3d_read_forces_end": (I, [P, C.POINTER(CellsForceSample), SZ, C.POINTER(SZ)]),
         "cells3d_read_status": (I, [P, C.POINTER(C.c_uint32)]),
+        "cells3d_check_diverged": (I, [P]),
         "cells3d_get_info": (I, [P, C.POINTER(Cells3DInfo)]),
         "cells3d_read_params": (I, [P, P]),
         "cells3d_mass": (I, [P, C.POINTER(D)]),
@@ -164,6 +165,7 @@ def lib() -> C.CDLL:
         "cells2d_read_forces_begin": (I, [P]),
         "cells2d_read_forces_end": (I, [P, C.POINTER(CellsForceSample), SZ, C.POINTER(SZ)]),
         "cells2d_read_status": (I, [P, C.POINTER(C.c_uint32)]),
+        "cells2d_check_diverged": (I, [P]),
         "cells2d_get_info": (I, [P, C.POINTER(Cells2DInfo)]),
         "cells2d_read_params": (I, [P, P]),
         "cells2d_mass": (I, [P, C.POINTER(D)]),
@@ -183,6 +185,7 @@ def lib() -> C.CDLL:
         "cells2d_batch_autotune": (I, [P, C.c_int32, C.POINTER(Cells2DInfo)]),
         "cells2d_batch_set_launch": (I, [P, C.c_int32, C.c_int32, C.c_int32]),
         "cells2d_batch_get_info": (I, [P, C.POINTER(Cells2DInfo)]),
+        "cells2d_batch_set_barrier_test": (I, [P, C.c_int32]),
         "cells2d_batch_timer_start": (I, [P]),
         "cells2d_batch_timer_stop": (I, [P, C.POINTER(C.c_float)]),
         "cells2d_batch_launch_count": (I, [P, C.POINTER(I64)]),

@@ -20,6 +20,8 @@ struct Step2Launch {
   int gridBlocks;                    // persistent launch: resident blocks
   unsigned* barrier;                 // persistent launch: grid barrier counter (zeroed per launch)
   int* error;                        // persistent launch: set to 1 when a barrier wait ran out
+  unsigned barrierExtra;             // persistent launch: arrivals added to every barrier's target
+                                     // (0; 1 only to test the time-out path)
 };
 
 // precision: 0 f32, 3 f64. fast: FMA contraction allowed; exact: every operation rounds as written.

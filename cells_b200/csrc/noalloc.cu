@@ -1,12 +1,11 @@
 // Allocation-free variant of the f64 mass reduction (cells3d_mass_noalloc in include/cells.h).
 //
-// Some callers cannot allocate device memory at the point where they need a result: code running
-// inside a CUDA stream capture (where cudaMalloc is not allowed), a host that owns a fixed memory
-// pool and forbids allocations after start-up, or a real-time loop that must not risk an
-// allocation failure or the implicit synchronisation cudaMalloc/cudaFree cause. This entry point
-// serves them: the caller passes the populations, the flags and a device location for the result,
-// and the per-block partial sums live in a file-scope __device__ array of fixed size instead of a
-// buffer the library allocates.
+// Some callers cannot allocate device memory at the point where they need a result: a host
+// application or plugin framework that owns every device buffer and forbids allocations after
+// start-up, or a real-time loop that must not risk an allocation failure or the implicit
+// synchronisation that cudaMalloc/cudaFree cause. This entry point serves them: the caller passes
+// the populations, the flags and a device location for the result, and the per-block partial sums
+// live in a file-scope __device__ array of fixed size instead of a buffer the library allocates.
 //
 // Limits and behaviour
 //   * the scratch holds 8192 doubles (64 KiB) on every GPU that loads the library, for the life of
@@ -18,7 +17,9 @@
 //   * all calls share the one array per device: calls that can overlap on the GPU (different
 //     streams, or different host threads) race on it and must be serialised by the caller;
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress) with
-//     that device current; make that first call before any stream capture that uses it.
+//     that device current and keeps it for that device's current CUDA context; make that first
+//     call before any stream capture that uses it. A call under a different context of the device
+//     (after a cudaDeviceReset, or with another context made current) looks the address up again.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -76,19 +77,42 @@ namespace {
 std::mutex g_scratch_mutex;
 constexpr int kMaxDevices = 64;
 double* g_scratch_ptr[kMaxDevices] = {nullptr};
+void* g_scratch_ctx[kMaxDevices] = {nullptr};  // the context each cached address belongs to
 
-// The device address of the scratch array on the current device, looked up once per device.
+// The driver's current context (cuCtxGetCurrent through the runtime's entry-point query, so the
+// library needs no link to libcuda); nullptr when it cannot be found, which disables caching.
+void* current_context() {
+  using GetCurrent = int (*)(void**);
+  static GetCurrent fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (GetCurrent) nullptr;
+    return (GetCurrent)f;
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+// The device address of the scratch array on the current device, looked up with that device
+// current and kept for the device's current context.
 cudaError_t scratch_on_current_device(double** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  // no current context yet (before the runtime's first use of the device): nullptr, and the
+  // address is looked up again on the next call
+  void* ctx = current_context();
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_ptr[dev]) {
+  if (!g_scratch_ptr[dev] || !ctx || g_scratch_ctx[dev] != ctx) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_mass_scratch);
     if (e != cudaSuccess) return e;
     g_scratch_ptr[dev] = (double*)p;
+    g_scratch_ctx[dev] = ctx;
   }
   *out = g_scratch_ptr[dev];
   return cudaSuccess;

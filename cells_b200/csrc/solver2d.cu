@@ -84,6 +84,8 @@ void validate_config(const Cells2DConfig& c) {
   if (c.left < 0 || c.left > 2 || c.right < 0 || c.right > 2) throw Error(CELLS_E_INVALID, "unknown x boundary mode");
   if (c.bottom < 0 || c.bottom > 3 || c.top < 0 || c.top > 3) throw Error(CELLS_E_INVALID, "unknown y boundary mode");
   if (c.force_every < 0) throw Error(CELLS_E_INVALID, "force_every must be >= 0");
+  if (c.workgroup_size != 0 && c.workgroup_size != 64 && c.workgroup_size != 128 && c.workgroup_size != 256)
+    throw Error(CELLS_E_INVALID, "workgroup_size must be 0, 64, 128 or 256");
 }
 
 }  // namespace
@@ -115,6 +117,7 @@ struct Cells2DBatch : HandleBase {
   uint64_t layoutGen = 1;
   bool useGraphs = true;
   unsigned barrierErrors = 0;
+  unsigned barrierExtra = 0;  // test hook: arrivals a persistent launch waits for that never come
 
   struct StepGraph {
     cudaGraphExec_t exec = nullptr;
@@ -318,6 +321,7 @@ void Cells2DBatch::launch_raw(int64_t n, int par, int allowSample) {
   a.allowSample = allowSample;
   a.barrier = dBarrier;
   a.error = dError;
+  a.barrierExtra = barrierExtra;
   a.gridBlocks = std::min(nTiles, persistentBlocks);
   const bool ex = arithmetic == CELLS_ARITH_EXACT;
   while (n > 0) {
@@ -366,6 +370,7 @@ void Cells2DBatch::build_graph(int allowSample, int par) {
   a.nSteps = 1;
   a.gridBlocks = 0;
   a.barrier = nullptr;
+  a.barrierExtra = 0;
   a.error = nullptr;
   const bool ex = arithmetic == CELLS_ARITH_EXACT;
   check_cuda(cudaStreamBeginCapture(dev.stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
@@ -418,6 +423,10 @@ void Cells2DBatch::check_barrier() {
   check_cuda(cudaMemcpy(&e, dError, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy error flag");
   if (e) {
     barrierErrors++;
+    // the flag is cleared so that later launches run; the tunnels stay part-stepped until the
+    // caller re-initialises them
+    dev.memset0(dError, sizeof(int));
+    dev.sync();
     throw Error(CELLS_E_TIMEOUT, "a grid barrier of the persistent step kernel timed out");
   }
 }
@@ -793,7 +802,8 @@ int cells2d_init_field(Cells2D* h, const float* macro4n) {
   }
   b->dev.sync();
   T.step = 0;
-  b->write_state(h->k, 1 | 2 | 4);
+  // a new flow clears the divergence status, as recoverFromBlowup's re-init starts over
+  b->write_state(h->k, 1 | 2 | 4 | 8);
   T.forceSamplesRead = 0;
   T.forceSteps.clear();
   T.forceGeneration++;
@@ -948,6 +958,20 @@ int cells2d_read_status(Cells2D* h, uint32_t* status) {
     if (e) s |= 4u;
   }
   *status = s;
+  C2_CATCH(h, kAllocPrefix)
+}
+
+int cells2d_check_diverged(Cells2D* h) {
+  if (!h) return CELLS_E_INVALID;
+  uint32_t st = 0;
+  const int rc = cells2d_read_status(h, &st);
+  if (rc != CELLS_OK) return rc;
+  if ((st & 3u) == 0) return CELLS_OK;
+  C2_TRY
+  std::string m = "the flow diverged:";
+  if (st & 1u) m += " a non-finite force sample";
+  if (st & 2u) m += (st & 1u) ? " and a non-finite macro value" : " a non-finite macro value";
+  throw Error(CELLS_E_DIVERGED, m);
   C2_CATCH(h, kAllocPrefix)
 }
 
@@ -1160,74 +1184,99 @@ int cells2d_batch_set_launch(Cells2DBatch* b, int32_t tile_x, int32_t tile_y, in
   C2_CATCH(b, kAllocPrefix)
 }
 
+int cells2d_batch_set_barrier_test(Cells2DBatch* b, int32_t extra_arrivals) {
+  if (!b) return CELLS_E_INVALID;
+  C2_TRY
+  if (extra_arrivals < 0 || extra_arrivals > 1) throw Error(CELLS_E_INVALID, "extra_arrivals must be 0 or 1");
+  b->dev.sync();
+  b->barrierExtra = (unsigned)extra_arrivals;
+  C2_CATCH(b, kAllocPrefix)
+}
+
 int cells2d_batch_autotune(Cells2DBatch* b, int32_t trial_steps, Cells2DInfo* info) {
   if (!b) return CELLS_E_INVALID;
   C2_TRY
   if (trial_steps <= 0) throw Error(CELLS_E_INVALID, "trial_steps must be positive");
   if (!b->dev.fake) {
     b->dev.sync();
-    // snapshot: the current populations and the device state of every tunnel
-    std::vector<void*> save;
-    for (Tunnel2Host& T : b->t) {
-      void* p = b->dev.alloc(9ull * b->bpp * (size_t)T.N + sizeof(DevState2), "autotune snapshot");
-      check_cuda(cudaMemcpyAsync(p, T.f[b->parity], 9ull * b->bpp * (size_t)T.N, cudaMemcpyDeviceToDevice,
-                                 b->dev.stream),
-                 "snapshot copy");
-      check_cuda(cudaMemcpyAsync((char*)p + 9ull * b->bpp * (size_t)T.N, T.st, sizeof(DevState2),
-                                 cudaMemcpyDeviceToDevice, b->dev.stream),
-                 "snapshot copy");
-      save.push_back(p);
-    }
     const int par0 = b->parity;
-    float best = 1e30f;
-    Shape2 bestShape = {b->tileX, b->tileY};
-    int bestPers = b->persistent;
-    const int warm = std::min(trial_steps, 20);
-    for (const Shape2& sh : kShapes) {
-      for (int pers = 0; pers <= 1; pers++) {
-        b->set_layout(sh.tx, sh.ty, pers);
-        if (pers && b->persistentBlocks <= 0) continue;
-        b->dev.memset0(b->dError, sizeof(int));
-        b->launch_raw(warm, par0, 0);
-        // a graph-replayed trial times the replay, not the capture: the layout change invalidated
-        // the step graphs, so they are rebuilt here, outside the timed region
-        if (!pers && b->useGraphs && trial_steps >= kGraphSteps2) {
-          b->build_graph(0, 0);
-          b->build_graph(0, 1);
-        }
-        check_cuda(cudaEventRecord(b->dev.ev0, b->dev.stream), "cudaEventRecord");
-        b->launch_raw(trial_steps, par0 ^ (warm & 1), 0);
-        check_cuda(cudaEventRecord(b->dev.ev1, b->dev.stream), "cudaEventRecord");
-        check_cuda(cudaEventSynchronize(b->dev.ev1), "cudaEventSynchronize");
-        float ms = 0.f;
-        check_cuda(cudaEventElapsedTime(&ms, b->dev.ev0, b->dev.ev1), "cudaEventElapsedTime");
-        int err = 0;
-        check_cuda(cudaMemcpy(&err, b->dError, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy error flag");
-        if (err) {
+    const int tx0 = b->tileX, ty0 = b->tileY, pers0 = b->persistent;
+    std::vector<void*> save;  // per tunnel: its populations and device state before the trials
+    // copies the snapshots back into the current parity's buffers and releases them
+    auto restore = [&]() {
+      for (size_t k = 0; k < save.size(); k++) {
+        Tunnel2Host& T = b->t[k];
+        check_cuda(cudaMemcpyAsync(T.f[par0], save[k], 9ull * b->bpp * (size_t)T.N, cudaMemcpyDeviceToDevice,
+                                   b->dev.stream),
+                   "restore copy");
+        check_cuda(cudaMemcpyAsync(T.st, (char*)save[k] + 9ull * b->bpp * (size_t)T.N, sizeof(DevState2),
+                                   cudaMemcpyDeviceToDevice, b->dev.stream),
+                   "restore copy");
+      }
+      b->dev.sync();
+      for (void* p : save) b->dev.release(p);
+      save.clear();
+      b->parity = par0;
+    };
+    try {
+      for (Tunnel2Host& T : b->t) {
+        void* p = b->dev.alloc(9ull * b->bpp * (size_t)T.N + sizeof(DevState2), "autotune snapshot");
+        save.push_back(p);
+        check_cuda(cudaMemcpyAsync(p, T.f[b->parity], 9ull * b->bpp * (size_t)T.N, cudaMemcpyDeviceToDevice,
+                                   b->dev.stream),
+                   "snapshot copy");
+        check_cuda(cudaMemcpyAsync((char*)p + 9ull * b->bpp * (size_t)T.N, T.st, sizeof(DevState2),
+                                   cudaMemcpyDeviceToDevice, b->dev.stream),
+                   "snapshot copy");
+      }
+      float best = 1e30f;
+      Shape2 bestShape = {b->tileX, b->tileY};
+      int bestPers = b->persistent;
+      const int warm = std::min(trial_steps, 20);
+      for (const Shape2& sh : kShapes) {
+        for (int pers = 0; pers <= 1; pers++) {
+          b->set_layout(sh.tx, sh.ty, pers);
+          if (pers && b->persistentBlocks <= 0) continue;
           b->dev.memset0(b->dError, sizeof(int));
-          continue;
-        }
-        if (ms < best) {
-          best = ms;
-          bestShape = sh;
-          bestPers = pers;
+          b->launch_raw(warm, par0, 0);
+          // a graph-replayed trial times the replay, not the capture: the layout change invalidated
+          // the step graphs, so they are rebuilt here, outside the timed region
+          if (!pers && b->useGraphs && trial_steps >= kGraphSteps2) {
+            b->build_graph(0, 0);
+            b->build_graph(0, 1);
+          }
+          check_cuda(cudaEventRecord(b->dev.ev0, b->dev.stream), "cudaEventRecord");
+          b->launch_raw(trial_steps, par0 ^ (warm & 1), 0);
+          check_cuda(cudaEventRecord(b->dev.ev1, b->dev.stream), "cudaEventRecord");
+          check_cuda(cudaEventSynchronize(b->dev.ev1), "cudaEventSynchronize");
+          float ms = 0.f;
+          check_cuda(cudaEventElapsedTime(&ms, b->dev.ev0, b->dev.ev1), "cudaEventElapsedTime");
+          int err = 0;
+          check_cuda(cudaMemcpy(&err, b->dError, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy error flag");
+          if (err) {
+            b->dev.memset0(b->dError, sizeof(int));
+            continue;
+          }
+          if (ms < best) {
+            best = ms;
+            bestShape = sh;
+            bestPers = pers;
+          }
         }
       }
+      b->set_layout(bestShape.tx, bestShape.ty, bestPers);
+      restore();
+    } catch (...) {
+      // a failed trial leaves the previous layout and the state before the call in place
+      try {
+        b->set_layout(tx0, ty0, pers0);
+        restore();
+      } catch (...) {
+        for (void* p : save) b->dev.release(p);
+        b->parity = par0;
+      }
+      throw;
     }
-    b->set_layout(bestShape.tx, bestShape.ty, bestPers);
-    // restore the snapshot into the current parity's buffers
-    for (size_t k = 0; k < b->t.size(); k++) {
-      Tunnel2Host& T = b->t[k];
-      check_cuda(cudaMemcpyAsync(T.f[par0], save[k], 9ull * b->bpp * (size_t)T.N, cudaMemcpyDeviceToDevice,
-                                 b->dev.stream),
-                 "restore copy");
-      check_cuda(cudaMemcpyAsync(T.st, (char*)save[k] + 9ull * b->bpp * (size_t)T.N, sizeof(DevState2),
-                                 cudaMemcpyDeviceToDevice, b->dev.stream),
-                 "restore copy");
-    }
-    b->dev.sync();
-    for (void* p : save) b->dev.release(p);
-    b->parity = par0;
   }
   if (info) {
     fill_info(b, b->t[0], info);

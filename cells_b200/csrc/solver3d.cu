@@ -521,7 +521,8 @@ int cells3d_init_field(Cells3D* h, const float* macro4n) {
     h->dev.launches++;
     if (macro4n) h->dev.sync();
   }
-  h->write_state(1 | 2);
+  // a new flow clears the divergence status, as recoverFromBlowup's re-init starts over
+  h->write_state(1 | 2 | 8);
   // resetForces (src/solver3d.ts:244-249)
   h->write_state(4);
   h->forceSamplesRead = 0;
@@ -659,6 +660,20 @@ int cells3d_read_status(Cells3D* h, uint32_t* status) {
   h->dev.d2h(h->stageState + 1, &h->st->status, sizeof(unsigned));
   h->dev.sync();
   *status = h->stageState[1];
+  CELLS_CATCH(h)
+}
+
+int cells3d_check_diverged(Cells3D* h) {
+  if (!h) return CELLS_E_INVALID;
+  uint32_t st = 0;
+  const int rc = cells3d_read_status(h, &st);
+  if (rc != CELLS_OK) return rc;
+  if (st == 0) return CELLS_OK;
+  CELLS_TRY(h)
+  std::string m = "the flow diverged:";
+  if (st & 1u) m += " a non-finite force sample";
+  if (st & 2u) m += (st & 1u) ? " and a non-finite macro value" : " a non-finite macro value";
+  throw Error(CELLS_E_DIVERGED, m);
   CELLS_CATCH(h)
 }
 

@@ -457,9 +457,17 @@ __global__ void __launch_bounds__(256, min_blocks2<C>()) step2d_kernel(const Tun
   tile2<C, ROWS>(tunnels, t, b - __ldg(&tunnels[t].firstTile), par, allowSample);
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Grid-wide barrier of the persistent kernel: arrivals count up a counter that the host zeroes
 // before each launch; barrier k of the launch waits for k * gridDim.x arrivals. The wait is
-// bounded (about a second); on time-out the block sets *error and the kernel winds down.
+// bounded by one second of the global timer and, as a backstop, by 2^23 polls; on time-out the
+// block sets *error and the kernel winds down (every other block's wait then ends at its next
+// poll).
 __device__ __forceinline__ bool grid_barrier2(unsigned* counter, unsigned target, int* error) {
   __shared__ int ok;
   __syncthreads();
@@ -468,11 +476,12 @@ __device__ __forceinline__ bool grid_barrier2(unsigned* counter, unsigned target
     __threadfence();
     atomicAdd(counter, 1u);
     long long spins = 0;
+    const unsigned long long t0 = global_ns();
     while (true) {
       unsigned seen;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(counter) : "memory");
       if (seen >= target) break;
-      if (*(volatile int*)error != 0 || ++spins > (1ll << 23)) {
+      if (*(volatile int*)error != 0 || ++spins > (1ll << 23) || global_ns() - t0 > 1000000000ull) {
         atomicExch(error, 1);
         ok = 0;
         break;
@@ -491,7 +500,7 @@ template <class C, int ROWS>
 __global__ void __launch_bounds__(256, min_blocks2<C>()) step2d_persistent_kernel(const Tunnel2* __restrict__ tunnels,
                                                                 const unsigned short* __restrict__ tileTunnel,
                                                                 int nTiles, int par, int nSteps, int allowSample,
-                                                                unsigned* barrier, int* error) {
+                                                                unsigned* barrier, int* error, unsigned extra) {
   for (int s = 0; s < nSteps; s++) {
     for (int b = blockIdx.x; b < nTiles; b += gridDim.x) {
       const int t = __ldg(&tileTunnel[b]);
@@ -499,7 +508,7 @@ __global__ void __launch_bounds__(256, min_blocks2<C>()) step2d_persistent_kerne
       __syncthreads();
     }
     par ^= 1;
-    if (s + 1 < nSteps && !grid_barrier2(barrier, (unsigned)(s + 1) * gridDim.x, error)) return;
+    if (s + 1 < nSteps && !grid_barrier2(barrier, (unsigned)(s + 1) * gridDim.x + extra, error)) return;
   }
 }
 
@@ -523,7 +532,8 @@ static cudaError_t launch_step2_persistent_t(const Step2Launch& a, cudaStream_t 
   int nTiles = a.nTiles, par = a.par, nSteps = a.nSteps, allowSample = a.allowSample;
   unsigned* barrier = a.barrier;
   int* error = a.error;
-  void* args[] = {&tunnels, &tileTunnel, &nTiles, &par, &nSteps, &allowSample, &barrier, &error};
+  unsigned extra = a.barrierExtra;
+  void* args[] = {&tunnels, &tileTunnel, &nTiles, &par, &nSteps, &allowSample, &barrier, &error, &extra};
   cudaError_t e = cudaMemsetAsync(barrier, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
   const void* fn = a.rows == 2 ? (const void*)step2d_persistent_kernel<C, 2> : (const void*)step2d_persistent_kernel<C, 1>;

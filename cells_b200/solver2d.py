@@ -215,6 +215,11 @@ class Solver:
         check(lib().cells2d_read_status(self._h, C.byref(s)), self._h)
         return s.value
 
+    def checkDiverged(self) -> None:
+        """Raises CellsError (status CELLS_E_DIVERGED) when a non-finite force sample or macro value
+        was seen on the device since the last initField."""
+        check(lib().cells2d_check_diverged(self._h), self._h)
+
     def readParams(self) -> bytes:
         buf = (C.c_uint8 * 96)()
         check(lib().cells2d_read_params(self._h, buf), self._h)
@@ -322,6 +327,12 @@ class Batch2D:
         i = _lib.Cells2DInfo()
         check(lib().cells2d_batch_get_info(self._h, C.byref(i)), self._h)
         return {k: getattr(i, k) for k, _ in i._fields_}
+
+    def setBarrierTest(self, extraArrivals: int) -> None:
+        """Test hook of the persistent kernel's time-out path: with 1, every grid barrier of later
+        persistent launches waits for an arrival that never comes, runs out after one second, and
+        the call that waits for the launch raises CellsError (CELLS_E_TIMEOUT); 0 restores it."""
+        check(lib().cells2d_batch_set_barrier_test(self._h, extraArrivals), self._h)
 
     def timerStart(self) -> None:
         check(lib().cells2d_batch_timer_start(self._h), self._h)

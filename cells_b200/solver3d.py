@@ -179,6 +179,11 @@ class Solver3D:
         check(lib().cells3d_read_status(self._h, C.byref(s)), self._h)
         return s.value
 
+    def checkDiverged(self) -> None:
+        """Raises CellsError (status CELLS_E_DIVERGED) when a non-finite force sample or macro value
+        was seen on the device since the last initField (src/tunnel3d.ts:97-105)."""
+        check(lib().cells3d_check_diverged(self._h), self._h)
+
     def readParams(self) -> bytes:
         buf = (C.c_uint8 * 64)()
         check(lib().cells3d_read_params(self._h, buf), self._h)

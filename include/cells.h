@@ -160,8 +160,14 @@ int cells3d_read_forces(Cells3D* h, CellsForceSample* out, size_t cap, size_t* n
  * generation check, src/solver3d.ts:298-304). */
 int cells3d_read_forces_begin(Cells3D* h);
 int cells3d_read_forces_end(Cells3D* h, CellsForceSample* out, size_t cap, size_t* n_out);
-/* Device-side status bits: 1 = a non-finite force sample, 2 = a non-finite macro value. */
+/* Device-side status bits: 1 = a non-finite force sample, 2 = a non-finite macro value. The word
+ * is cleared at create and by init_field. */
 int cells3d_read_status(Cells3D* h, uint32_t* status);
+/* The divergence checks of the reference's pages (hasDiverged / fieldDiverged,
+ * src/tunnel3d.ts:97-105: a non-finite force sample or macro value), answered from the device-side
+ * status word instead of a scan of the read-back samples: CELLS_OK, or CELLS_E_DIVERGED with the
+ * reason in cells_last_error. Waits for the stream. */
+int cells3d_check_diverged(Cells3D* h);
 int cells3d_get_info(Cells3D* h, Cells3DInfo* info);
 /* The 64-byte Params3 block exactly as the reference packs it (src/shaders/common3d.ts:9-16,
  * src/solver3d.ts:197-208): u32 W,H,D,N,groupsX,0,0,0; f32 tau, lambda, smagC2, uIn,
@@ -190,16 +196,19 @@ int cells3d_sample_slice(Cells3D* h, int axis, double pos, int mode, double u_re
 int cells3d_advect_tracers(Cells3D* h, const float* seeds, float* particles, int count, double steps, double u_ref);
 
 /* Allocation-free mass reduction. It has no counterpart in the reference. It is for callers that
- * cannot allocate device memory when they need the result: code inside a CUDA stream capture,
- * hosts that fix their device memory at start-up, real-time loops that must not risk the failure
- * or the implicit synchronisation of cudaMalloc/cudaFree. The caller passes device pointers to
+ * cannot allocate device memory when they need the result: host applications or plugin frameworks
+ * that own every device buffer and fix their device memory at start-up, and real-time loops that
+ * must not risk the failure or the implicit synchronisation of cudaMalloc/cudaFree. The array it
+ * uses is held by every GPU that loads the library until the process exits. The caller passes device pointers to
  * the populations (19 * n_cells values of the storage type, layout f[i * n_cells + cell]) and to
  * the flags (n_cells u32), a device pointer for the f64 result, and a CUDA stream (NULL = the
  * default stream); the call enqueues the work and returns without waiting. The partial sums live in
  * a fixed 64 KiB __device__ array, one partial per 8192 cells: grids above 67,108,864 cells are
  * rejected with CELLS_E_INVALID. Calls share that array, so calls that can overlap on the GPU
- * race and must be serialised by the caller. The first call on a device looks up the array's
- * address and should come before any stream capture. Errors: cells_last_error(NULL). */
+ * race and must be serialised by the caller; the array keeps the last call's partial sums, and
+ * every call overwrites each partial it reads. The first call on a device (and the first under a
+ * new context of it, e.g. after cudaDeviceReset) looks up the array's address; that first call
+ * should come before any stream capture. Errors: cells_last_error(NULL). */
 int cells3d_mass_noalloc(const void* populations, const uint32_t* flags, int64_t n_cells, int32_t precision,
                          double* out_device, void* stream);
 
@@ -360,8 +369,12 @@ int cells2d_read_macro(Cells2D* h, float* out4n);
 int cells2d_read_forces(Cells2D* h, CellsForceSample* out, size_t cap, size_t* n_out);
 int cells2d_read_forces_begin(Cells2D* h);
 int cells2d_read_forces_end(Cells2D* h, CellsForceSample* out, size_t cap, size_t* n_out);
-/* bits: 1 non-finite force sample, 2 non-finite macro value, 4 a persistent-launch barrier timed out */
+/* bits: 1 non-finite force sample, 2 non-finite macro value (both cleared by init_field), 4 a
+ * persistent-launch barrier timed out */
 int cells2d_read_status(Cells2D* h, uint32_t* status);
+/* CELLS_OK, or CELLS_E_DIVERGED when status bit 1 or 2 is set (hasDiverged / fieldDiverged of
+ * src/tunnel3d.ts:97-105, as the 2D page applies them, src/app.ts:433-460). */
+int cells2d_check_diverged(Cells2D* h);
 int cells2d_get_info(Cells2D* h, Cells2DInfo* info);
 /* The 96-byte Params block as the reference packs it (src/shaders/common.ts:14-22,
  * src/solver.ts:180-197). */
@@ -397,6 +410,12 @@ int cells2d_batch_autotune(Cells2DBatch* b, int32_t trial_steps, Cells2DInfo* in
  * thread) when the batch has 4,096 tiles or more at one row per thread. */
 int cells2d_batch_set_launch(Cells2DBatch* b, int32_t tile_x, int32_t tile_y, int32_t persistent);
 int cells2d_batch_get_info(Cells2DBatch* b, Cells2DInfo* info);
+/* Test hook of the persistent kernel's time-out path: with extra_arrivals = 1 every grid barrier of
+ * the following persistent launches waits for one arrival that never comes, so the bounded wait
+ * (one second) runs out, the kernel winds down, and the call that waits for it returns
+ * CELLS_E_TIMEOUT and clears the device error flag; the tunnels are then part-stepped until they
+ * are re-initialised. 0 (the default) restores normal barriers. */
+int cells2d_batch_set_barrier_test(Cells2DBatch* b, int32_t extra_arrivals);
 int cells2d_batch_timer_start(Cells2DBatch* b);
 int cells2d_batch_timer_stop(Cells2DBatch* b, float* ms);
 int cells2d_batch_launch_count(Cells2DBatch* b, int64_t* count);

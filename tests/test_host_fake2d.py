@@ -104,6 +104,12 @@ def test_bad_configs():
         fake(width=1)
     with pytest.raises(_lib.CellsError):
         fake(top=7)
+    for wg in (32, 96, 512):
+        with pytest.raises(_lib.CellsError) as e:
+            fake(workgroupSize=wg)
+        assert e.value.status == _lib.CELLS_E_INVALID
+    for wg in (0, 64, 128, 256):
+        fake(workgroupSize=wg).destroy()
 
 
 def test_batch_rules():

@@ -1,7 +1,7 @@
 """cells3d_mass_noalloc, the allocation-free mass reduction, against the handle's cells3d_mass.
 
-Callers that cannot allocate device memory (inside a stream capture, with a fixed memory pool, in
-a real-time loop) pass their own device buffers; this test plays such a caller. torch only holds
+Callers that cannot allocate device memory (a host or plugin framework that owns every device
+buffer, a real-time loop) pass their own device buffers; this test plays such a caller. torch only holds
 the caller's device buffers here. The two reductions sum the same f64 values in different orders,
 so they agree to 1e-12 relative. The file name sorts last so that a run stopping at the first
 failure has already run every other test.
@@ -32,7 +32,7 @@ def noalloc_mass(torch, pops, flags, n, precision, out, stream):
     return rc
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+@pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16", "fp64"])
 def test_noalloc_mass_matches_handle_mass_twice(precision):
     torch = pytest.importorskip("torch")
     W, H, D = 48, 24, 24

@@ -11,6 +11,7 @@ One step = one fused step kernel over the whole grid. The two distribution buffe
 exceed the 126 MB L2, so every timed step streams from HBM without an explicit flush.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --precision-sweep    (sphere, cube, spanwise cylinder, NACA wing x FP32/FP16/BF16)
 
 With --gpus N under torchrun every rank runs an independent replica on its own GPU (the path does
 not shard: replicas only); value is the whole-job MLUPS from the max time over ranks.
@@ -53,58 +54,75 @@ def profiled_traffic(workload: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    """SM clocks and throttle reasons read through NVML (read-only queries) while the timed region
+    runs: one sample as it starts, one every 2 ms from a thread, one as it ends, so even a
+    millisecond-long region has samples taken during it."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.proc = None
-        self.path = None
+        self.samples = []
+        self.nv = None
+        self.handle = None
+        self.thread = None
+        self.stop = None
+
+    def _sample(self):
+        nv, h = self.nv, self.handle
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.samples.append((sm, smax, bits))
+        except Exception:
+            pass
+
+    def _loop(self):
+        while not self.stop.wait(0.002):
+            self._sample()
 
     def __enter__(self):
+        import threading
+
         try:
-            fd, self.path = tempfile.mkstemp(suffix=".csv")
-            os.close(fd)
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
-                 "-i", str(self.gpu), "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self.nv = nv
+            self.handle = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            self._sample()
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._loop, daemon=True)
+            self.thread.start()
         except Exception:
-            self.proc = None
+            self.nv = None
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
+        if self.nv is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            self._sample()
             try:
-                self.proc.wait(timeout=5)
+                self.nv.nvmlShutdown()
             except Exception:
-                self.proc.kill()
+                pass
 
     def summary(self):
-        if not self.path or not os.path.exists(self.path):
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        os.unlink(self.path)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = set()
+        for _, _, bits in self.samples:
+            for name, attr in self.REASONS:
+                if bits & getattr(self.nv, attr, 0):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(x[0] for x in self.samples),
+                "sm_max_mhz": max(x[1] for x in self.samples), "reasons": sorted(reasons),
+                "samples": len(self.samples), "source": "NVML, 2 ms period plus the start and end of the region"}
 
 
 def physical_gpu_index(local_rank: int) -> int:
@@ -220,13 +238,17 @@ def precision_cd(device, steps=5000, grid=(192, 96, 96)):
 
 def adjoint_cost(device):
     """Wall time of the adjoint's backward sweep (recompute + adjoint steps) over one plain forward
-    run of the same 6000 steps, on the 128x64x64 star-body drag problem (FP32)."""
+    run of the same 6000 steps, on the 128x64x64 star-body drag problem (FP32): cost_ratio is the
+    sweep alone; total_gradient_ratio adds the recording forward run (which also sets the SDF and
+    the link tables) that the gradient needs."""
     from cells_b200.adjoint import StarDrag
     from cells_b200.rng import SEED, normal
 
     p = StarDrag(precision="fp32", device=device)
-    J = p.forward(0.02 * normal(SEED, 17, 16))
+    t0 = time.perf_counter()
+    J = p.forward(0.02 * normal(SEED, 17, 16))  # the recording forward run (checkpoints every 100 steps)
     p.solver.synchronize()
+    t_rec = time.perf_counter() - t0
     t0 = time.perf_counter()
     r = p.solver.adjointBackward()  # the sweep: recompute from checkpoints + adjoint steps
     t_bwd = time.perf_counter() - t0
@@ -243,8 +265,8 @@ def adjoint_cost(device):
     t_fwd = time.perf_counter() - t0
     p.destroy()
     return {"workload": "star body r0=12 at 128x64x64, Re150, 6000 steps, K=100, FP32", "J": J,
-            "forward_s": t_fwd, "backward_s": t_bwd, "cost_ratio": t_bwd / t_fwd, "chain_rule_s": t_chain,
-            "dJ_du": du}
+            "forward_s": t_fwd, "recording_forward_s": t_rec, "backward_s": t_bwd, "cost_ratio": t_bwd / t_fwd,
+            "total_gradient_ratio": (t_rec + t_bwd) / t_fwd, "chain_rule_s": t_chain, "dJ_du": du}
 
 
 def cpu_baseline(W, H, D, precision="fp32", budget_s=12.0, max_steps=400):
@@ -294,7 +316,17 @@ def main():
     ap.add_argument("--profile2d", action="store_true",
                     help="short run for ncu of the 2D step kernel: the 64 batched NACA tunnels, one launch per "
                          "step (tile 32 x 2), warmup + steps")
+    ap.add_argument("--precision-sweep", action="store_true",
+                    help="the four-obstacle precision sweep at 256x128x128 (FP32, FP16, BF16 against FP64 on the same "
+                         "grid and on 128x64x64); prints one JSON line and a markdown table")
     args = ap.parse_args()
+    if args.precision_sweep:
+        from cells_b200 import cases3d
+
+        rows = cases3d.precision_sweep()
+        print(json.dumps({"precision_sweep": rows}), flush=True)
+        print(cases3d.sweep_table(rows), flush=True)
+        return
     if args.profile_adjoint:
         from cells_b200.adjoint import StarDrag
         from cells_b200.rng import SEED, normal
@@ -391,29 +423,36 @@ def main():
         "clocks": clk,
     }
     if not args.no_extras and not args.profile:
-        e2e_steps = min(args.steps, 1000)
+        e2e_steps = 1000  # fixed: the public-API loop of 10 chunks of 100 steps, whatever --steps is
         dt, h2d, d2h = run_e2e(s, sdf, macro, e2e_steps)
         line["e2e"] = {"value": round(N * e2e_steps / dt / 1e6 * world, 1), "unit": "MLUPS",
                        "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
                        "steps": e2e_steps, "calls": "setSdf, initField, (setInlet, run(100), readForces) x k, readMacro"}
         s.destroy()
-        variants = []
-        for prec, grid in (("fp16", (W, H, D)), ("bf16", (W, H, D)), ("fp64", (W, H, D)),
-                           ("fp32", (256, 128, 128)), ("fp16", (256, 128, 128))):
+        def variant(prec, grid, steps):
             v, vsdf, vmac, _ = tunnel_setup(*grid, prec, device=local)
             v.setSdf(vsdf)
             v.initField(vmac)
             v.setInletRamp("linear", 0.1, 3000, 1)
-            vms, _ = time_steps(v, 50, 500)
-            vn = grid[0] * grid[1] * grid[2]
-            vm = vn * 500 / (vms * 1e3)
-            vcopy = copy_roofline(local, prec, vn)
-            variants.append({"storage": prec, "grid": list(grid), "mlups": round(vm, 1),
-                             "hbm_frac": round(vm * 1e6 * BYTES_PER_CELL[prec] / 1e9 / hbm, 4),
-                             "copy_gbps": vcopy["gbps"],
-                             "copy_frac": round(vm * 1e6 * BYTES_PER_CELL[prec] / 1e9 / vcopy["gbps"], 4)})
+            vms, _ = time_steps(v, 100, steps)
             v.destroy()
-        line["variants"] = variants
+            vn = grid[0] * grid[1] * grid[2]
+            vm = vn * steps / (vms * 1e3)
+            vcopy = copy_roofline(local, prec, vn)
+            return {"storage": prec, "grid": list(grid), "steps": steps, "mlups": round(vm, 1),
+                    "hbm_frac": round(vm * 1e6 * BYTES_PER_CELL[prec] / 1e9 / hbm, 4),
+                    "copy_gbps": vcopy["gbps"],
+                    "copy_frac": round(vm * 1e6 * BYTES_PER_CELL[prec] / 1e9 / vcopy["gbps"], 4)}
+
+        line["variants"] = [variant(prec, (W, H, D), 1000) for prec in ("fp16", "bf16", "fp64")]
+        # the targets' own workload: the 256x128x128 step in FP32 and 16-bit storage, CUDA events
+        big = {prec: variant(prec, (256, 128, 128), 2000) for prec in ("fp32", "fp16", "bf16")}
+        line["north_star_256x128x128"] = {
+            "workload": "D3Q19 256x128x128 sphere tunnel (d = 21.3, Re 200), 2000 timed steps after 100",
+            "fp32": big["fp32"], "fp16": big["fp16"], "bf16": big["bf16"],
+            "fp16_over_fp32": round(big["fp16"]["mlups"] / big["fp32"]["mlups"], 4),
+            "bf16_over_fp32": round(big["bf16"]["mlups"] / big["fp32"]["mlups"], 4),
+            "targets": "HBM frac >= 0.75 in FP32 and FP16; FP16 >= 1.8x FP32"}
         from cells_b200 import cases2d
 
         line["precision_cd"] = precision_cd(local)

@@ -359,7 +359,9 @@ def batched_naca_throughput(steps: int = 10000, device: int = 0, autotune: bool 
                             count: int = 64) -> dict:
     """MLUPS of the batched tunnels stepped together (one Batch2D, CUDA-graph or persistent
     launches as the autotuner picks) and of the same tunnels stepped one at a time (one Solver
-    each, graph-replayed), both timed with CUDA events on the solvers' streams."""
+    each, graph-replayed), both timed with CUDA events on the solvers' streams; the final
+    populations of each tunnel, batched and alone, are compared (how many are bit for bit equal,
+    and the largest difference)."""
     from .solver2d import Batch2D
 
     tunnels = batched_naca_tunnels(count)
@@ -374,10 +376,11 @@ def batched_naca_throughput(steps: int = 10000, device: int = 0, autotune: bool 
     b.timerStart()
     b.step(steps)
     ms_batch = b.timerStop()
-    ok = all(np.all(np.isfinite(t.readPopulations()[: 9 * 64])) for t in b.tunnels[:4])
+    batched = [t.readPopulations() for t in b.tunnels]
     b.destroy()
     ms_seq = 0.0
-    for c, sdf in tunnels:
+    identical, max_diff = 0, 0.0
+    for (c, sdf), fb in zip(tunnels, batched):
         s = Solver.create(device=device, **c)
         s.setSdf(sdf)
         s.initField(perturbed_rest2(c["width"], c["height"], 1e-4))
@@ -386,10 +389,16 @@ def batched_naca_throughput(steps: int = 10000, device: int = 0, autotune: bool 
         s.timerStart()
         s.encodeSteps(steps)
         ms_seq += s.timerStop()
+        fs = s.readPopulations()
         s.destroy()
+        # the same tunnel after the same steps, batched and alone
+        identical += int(np.array_equal(fb.view(np.uint32), fs.view(np.uint32)))
+        max_diff = max(max_diff, float(np.max(np.abs(fb.astype(np.float64) - fs.astype(np.float64)))))
     return {"tunnels": count, "cells": cells, "steps": steps, "batched_mlups": cells * steps / (ms_batch * 1e3),
             "sequential_mlups": cells * steps / (ms_seq * 1e3), "speedup": ms_seq / ms_batch,
-            "batched_ms": ms_batch, "sequential_ms": ms_seq, "finite": bool(ok),
+            "batched_ms": ms_batch, "sequential_ms": ms_seq,
+            "bitwise_identical_tunnels": identical, "max_population_diff": max_diff,
+            "finite": bool(all(np.all(np.isfinite(f)) for f in batched)),
             "launch": {"tile": [launch["tile_x"], launch["tile_y"]], "persistent": bool(launch["persistent"])}}
 
 

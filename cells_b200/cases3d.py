@@ -130,3 +130,24 @@ def precision_sweep(device=0, grid=(256, 128, 128), steps=4000, obstacles=OBSTAC
         row["seconds"] = time.perf_counter() - t0
         out.append(row)
     return out
+
+
+def sweep_table(rows) -> str:
+    """The precision sweep as a markdown table: per obstacle and storage, C_D and C_L (mean over the
+    second half of the run), the relative C_D error and absolute C_L error against the FP64 run on
+    the same grid, the relative C_D difference to the FP64 run on the half grid, and the relative
+    velocity L2 difference at the last step."""
+    out = ["| obstacle | storage | C_D | C_L | C_D err vs FP64 | C_L abs err vs FP64 | C_D vs FP64 half grid "
+           "| velocity L2 vs FP64 |", "|---|---|---|---|---|---|---|---|"]
+    for r in rows:
+        out.append(f"| {r['obstacle']} ({r['size']:g}) | FP64 | {r['fp64']['C_D']:.5f} | {r['fp64']['C_L']:.5f} "
+                   f"| — | — | {abs(r['fp64']['C_D'] - r['fp64_half_grid']['C_D']) / abs(r['fp64_half_grid']['C_D']):.2e} "
+                   f"| — |")
+        for prec in ("fp32", "fp16", "bf16"):
+            if prec not in r:
+                continue
+            e = r[prec]
+            out.append(f"| | {prec.upper()} | {e['C_D']:.5f} | {e['C_L']:.5f} | {e['C_D_err_vs_fp64']:.2e} "
+                       f"| {e['C_L_abs_err_vs_fp64']:.2e} | {e['C_D_err_vs_fp64_half_grid']:.2e} "
+                       f"| {e['vel_L2_vs_fp64']:.2e} |")
+    return "\n".join(out)

@@ -487,12 +487,9 @@ void release_adjoint(Cells3D* h) {
   Adjoint3D* A = h->adj.get();
   std::vector<void*> ptrs = {A->endState, A->linkBase, A->le1, A->le2, A->la1, A->la2, A->lcF, A->lq, A->lqk,
                              A->lamG, A->dqAcc, A->rowElem, A->rowSet, A->rowStart, A->entLink, A->entAlpha,
-                             A->rowPhi, A->lam[0], A->lam[1], A->blockPart, A->counter, A->dudn,
-                             A->slowCells, A->sE1, A->sE2, A->sTgt, A->sA1, A->sA2};
-  for (void* p : A->ck) ptrs.push_back(p);
-  for (void* p : A->ckState) ptrs.push_back(p);
-  for (int k = 0; k < 2; k++)
-    for (void* p : A->seg[k]) ptrs.push_back(p);
+                             A->rowPhi, A->blockPart, A->counter, A->dudn,
+                             A->slowCells, A->sE1, A->sE2, A->sTgt, A->sA1, A->sA2, A->ckStateBlock};
+  // the checkpoints, recompute buffers and adjoint states live in h->adjStore, which stays
   ptrs.push_back(A->uDev);
   ptrs.push_back(A->wDev);
   ptrs.push_back(A->n0Dev);
@@ -538,30 +535,50 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
     int link;  // -1: no regular reader; -2: a force term
     double alpha;
   };
-  std::vector<Ent> ents;
-  ents.reserve(L.size() * 3);
+  // the links' entries, sorted by element (ties keep their order of insertion: link order, then
+  // e1, e2, force within a link)
+  std::vector<Ent> lent;
+  lent.reserve(L.size() * 3);
   for (int k = 0; k < A->nLinks; k++) {
-    ents.push_back({L[k].e1, k, L[k].a1});
-    if (L[k].e2 >= 0) ents.push_back({L[k].e2, k, L[k].a2});
-    if (L[k].cF != 0.0) ents.push_back({L[k].e1, -2, L[k].cF});
+    lent.push_back({L[k].e1, k, L[k].a1});
+    if (L[k].e2 >= 0) lent.push_back({L[k].e2, k, L[k].a2});
+    if (L[k].cF != 0.0) lent.push_back({L[k].e1, -2, L[k].cF});
   }
+  std::vector<std::pair<long long, int>> key(lent.size());
+  for (size_t p = 0; p < lent.size(); p++) key[p] = {lent[p].e, (int)p};
+  std::sort(key.begin(), key.end());
+  // elements without a regular reader, generated in increasing element order (direction outer)
   auto at = [&](int x, int y, int z) { return (long long)x + (long long)W * ((long long)y + (long long)H * z); };
-  for (int z = 0; z < D; z++)
-    for (int y = 0; y < H; y++)
-      for (int x = 0; x < W; x++) {
-        const long long c = at(x, y, z);
-        if (fl[(size_t)c] & FLAG3_SOLID) continue;
-        for (int i = 0; i < Q3; i++) {
-          const int rx = x + cx3(i), ry = y + cy3(i), rz = z + cz3(i);
-          bool regular = rx >= 0 && rx < W && ry >= 0 && ry < H && rz >= 0 && rz < D;
+  std::vector<long long> irregular;
+  for (int i = 0; i < Q3; i++)
+    for (int z = 0; z < D; z++)
+      for (int y = 0; y < H; y++) {
+        const int ry = y + cy3(i), rz = z + cz3(i);
+        const bool rowIn = ry >= 0 && ry < H && rz >= 0 && rz < D;
+        for (int x = 0; x < W; x++) {
+          const long long c = at(x, y, z);
+          if (fl[(size_t)c] & FLAG3_SOLID) continue;
+          const int rx = x + cx3(i);
+          bool regular = rowIn && rx >= 0 && rx < W;
           if (regular) {
             const uint32_t g = fl[(size_t)at(rx, ry, rz)];
             regular = !(g & (FLAG3_SOLID | FLAG3_INLET)) && (i == 0 || !(g & (1u << i)));
           }
-          if (!regular) ents.push_back({i * N + c, -1, 0.0});
+          if (!regular) irregular.push_back(i * N + c);
         }
       }
-  std::stable_sort(ents.begin(), ents.end(), [](const Ent& a, const Ent& b) { return a.e < b.e; });
+  // merge: for one element the link entries come before its no-reader mark
+  std::vector<Ent> ents;
+  ents.reserve(lent.size() + irregular.size());
+  {
+    size_t p = 0, q = 0;
+    while (p < key.size() || q < irregular.size()) {
+      if (q >= irregular.size() || (p < key.size() && key[p].first <= irregular[q]))
+        ents.push_back(lent[(size_t)key[p++].second]);
+      else
+        ents.push_back({irregular[q++], -1, 0.0});
+    }
+  }
   std::vector<long long> rowElem;
   std::vector<unsigned char> rowSet;
   std::vector<int> rowStart, entLink;
@@ -894,20 +911,34 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
   const size_t fBytes = 19ull * h->bpp * (size_t)h->N;
   const int64_t nSeg = (A->steps + A->K - 1) / A->K;
   const int segBufs = (int)std::min<int64_t>(A->K, A->steps);
-  const size_t need = (size_t)(nSeg + 2 * segBufs + 2) * fBytes + (size_t)h->N * 16;
-  if (need > dev.free_bytes())
-    throw AllocError("the adjoint's checkpoints need " + std::to_string(need) + " bytes; the device has " +
-                     std::to_string(dev.free_bytes()) + " free");
+  // one block for the checkpoints, both sets of recompute buffers and both adjoint states, each
+  // at a 256-byte aligned stride; kept for the next recorded run while it fits
+  const size_t stride = (fBytes + 255) / 256 * 256;
+  const size_t need = (size_t)(nSeg + 2 * segBufs + 2) * stride;
+  if (!h->adjStore || h->adjStoreBytes < need) {
+    if (h->adjStore) {
+      dev.release(h->adjStore);
+      h->adjStore = nullptr;
+      h->adjStoreBytes = 0;
+    }
+    if (need + (size_t)h->N * 16 > dev.free_bytes())
+      throw AllocError("the adjoint's checkpoints need " + std::to_string(need) + " bytes; the device has " +
+                       std::to_string(dev.free_bytes()) + " free");
+    h->adjStore = dev.alloc(need, "adjoint checkpoints");
+    h->adjStoreBytes = need;
+  }
   build_tables(h, A);
+  char* store = (char*)h->adjStore;
+  A->ckStateBlock = (DevState3*)dev.alloc((size_t)nSeg * sizeof(DevState3), "adjoint checkpoint");
   for (int64_t k = 0; k < nSeg; k++) {
-    A->ck.push_back(dev.alloc(fBytes, "adjoint checkpoint"));
-    A->ckState.push_back(dev.alloc(sizeof(DevState3), "adjoint checkpoint"));
+    A->ck.push_back(store + (size_t)k * stride);
+    A->ckState.push_back(A->ckStateBlock + k);
   }
   for (int set = 0; set < 2; set++)
-    for (int k = 0; k < segBufs; k++) A->seg[set].push_back(dev.alloc(fBytes, "adjoint segment"));
+    for (int k = 0; k < segBufs; k++) A->seg[set].push_back(store + (size_t)(nSeg + set * segBufs + k) * stride);
   A->endState = dev.alloc(sizeof(DevState3), "adjoint end state");
-  A->lam[0] = dev.alloc(fBytes, "adjoint state");
-  A->lam[1] = dev.alloc(fBytes, "adjoint state");
+  A->lam[0] = store + (size_t)(nSeg + 2 * segBufs) * stride;
+  A->lam[1] = store + (size_t)(nSeg + 2 * segBufs + 1) * stride;
   // 32-cell x tiles: each warp still reads 128-byte rows, and the tiles before the absorbing layer
   // take the collision code without it
   A->tileX = 32;
@@ -935,22 +966,69 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
     const int64_t s = s0 + n;
     A->uStep[(size_t)n] = h->uin_at(s);
     A->rampStep[(size_t)n] = h->rampKind ? (h->rampTarget != 0.0 ? h->ramp_speed(s) / h->rampTarget : 0.0) : 1.0;
-    if (n % A->K == 0) {
-      const int64_t k = n / A->K;
-      check_cuda(cudaMemcpyAsync(A->ck[(size_t)k], h->f[h->parity], fBytes, cudaMemcpyDeviceToDevice, dev.stream),
-                 "checkpoint copy");
-      check_cuda(cudaMemcpyAsync(A->ckState[(size_t)k], h->st, sizeof(DevState3), cudaMemcpyDeviceToDevice,
-                                 dev.stream),
-                 "checkpoint copy");
-    }
-    const int64_t label = s + 1;
-    const bool sample = label >= A->w0 && label <= A->w1;
-    h->enqueue_step_between(h->f[h->parity], h->f[h->parity ^ 1], h->parity, sample);
-    dev.launches++;
-    h->parity ^= 1;
-    h->step++;
-    if (sample) h->forceSteps.push_back((uint32_t)h->step);
   }
+  // Segments of K steps (K even) that are all sampled or all unsampled replay a graph of K steps
+  // captured once per recorded run: with K even every segment starts at the parity of the first.
+  cudaGraphExec_t recGraph[2] = {nullptr, nullptr};  // [sampled]
+  int64_t recGraphLaunches[2] = {0, 0};
+  const bool recGraphs = h->useGraphs && A->K % 2 == 0;
+  auto record_graph = [&](int sampled) {
+    const int64_t before = dev.launches;
+    const int p0 = h->parity;
+    check_cuda(cudaStreamBeginCapture(dev.stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    for (int t = 0; t < A->K; t++) {
+      const int p = p0 ^ (t & 1);
+      h->enqueue_step_between(h->f[p], h->f[p ^ 1], p, sampled != 0);
+      dev.launches++;
+    }
+    cudaGraph_t graph = nullptr;
+    check_cuda(cudaStreamEndCapture(dev.stream, &graph), "cudaStreamEndCapture");
+    const cudaError_t e = cudaGraphInstantiate(&recGraph[sampled], graph, 0);
+    cudaGraphDestroy(graph);
+    check_cuda(e, "cudaGraphInstantiate");
+    recGraphLaunches[sampled] = dev.launches - before;
+    dev.launches = before;
+  };
+  try {
+    for (int64_t n = 0; n < A->steps;) {
+      if (n % A->K == 0) {
+        const int64_t k = n / A->K;
+        check_cuda(cudaMemcpyAsync(A->ck[(size_t)k], h->f[h->parity], fBytes, cudaMemcpyDeviceToDevice, dev.stream),
+                   "checkpoint copy");
+        check_cuda(cudaMemcpyAsync(A->ckState[(size_t)k], h->st, sizeof(DevState3), cudaMemcpyDeviceToDevice,
+                                   dev.stream),
+                   "checkpoint copy");
+        const int64_t first = s0 + n + 1, last = s0 + n + A->K;  // the segment's step labels
+        const bool all = first >= A->w0 && last <= A->w1, none = last < A->w0 || first > A->w1;
+        if (recGraphs && n + A->K <= A->steps && (all || none)) {
+          const int sampled = all ? 1 : 0;
+          if (!recGraph[sampled]) record_graph(sampled);
+          check_cuda(cudaGraphLaunch(recGraph[sampled], dev.stream), "cudaGraphLaunch");
+          dev.launches += recGraphLaunches[sampled];
+          for (int t = 0; t < A->K; t++) {
+            h->step++;
+            if (all) h->forceSteps.push_back((uint32_t)h->step);
+          }
+          n += A->K;
+          continue;
+        }
+      }
+      const int64_t label = s0 + n + 1;
+      const bool sample = label >= A->w0 && label <= A->w1;
+      h->enqueue_step_between(h->f[h->parity], h->f[h->parity ^ 1], h->parity, sample);
+      dev.launches++;
+      h->parity ^= 1;
+      h->step++;
+      if (sample) h->forceSteps.push_back((uint32_t)h->step);
+      n++;
+    }
+  } catch (...) {
+    for (cudaGraphExec_t g : recGraph)
+      if (g) cudaGraphExecDestroy(g);
+    throw;
+  }
+  for (cudaGraphExec_t g : recGraph)
+    if (g) cudaGraphExecDestroy(g);
   check_cuda(cudaMemcpyAsync(A->endState, h->st, sizeof(DevState3), cudaMemcpyDeviceToDevice, dev.stream),
              "end state copy");
   // the objective from the window's samples (ring slots written0 .. written0 + nWin - 1)
@@ -1067,6 +1145,11 @@ int cells3d_adjoint_release(Cells3D* h) {
   if (!h) return CELLS_E_INVALID;
   ADJ_TRY(h)
   release_adjoint(h);
+  if (h->adjStore) {
+    h->dev.release(h->adjStore);
+    h->adjStore = nullptr;
+    h->adjStoreBytes = 0;
+  }
   ADJ_CATCH(h)
 }
 

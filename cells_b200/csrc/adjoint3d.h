@@ -44,8 +44,9 @@ struct Adjoint3D {
   std::vector<double> rampStep; // d u_n / d u_in of each recorded step
 
   // checkpoints: the populations and device state at the start of every segment
-  std::vector<void*> ck;
-  std::vector<void*> ckState;
+  std::vector<void*> ck;       // into the handle's adjStore
+  std::vector<void*> ckState;  // into ckStateBlock
+  cells::DevState3* ckStateBlock = nullptr;
   void* endState = nullptr;  // device state after the run (restored after the backward sweep)
   std::vector<void*> seg[2];  // two sets of K recomputed states: the segment being swept and the next
 

@@ -93,6 +93,21 @@ void Cells3D::upload_xtab() {
     fill_xtab<float>(t, W, cfg.tau, lambda_value(), sponge_start(), tau_sponge(), cfg.absorb);
     for (int x = W - 1; x >= 0; x--)
       if (t[4 * x + 2] > 0.0f) firstAbsorb = x;
+    // the x-pair layout of the same values after the W per-x entries: entry x0 (even) holds
+    // (omega+ of x0, of x0 + 1, omega- of x0, of x0 + 1), entry x0 + 1 (sigma of x0, of x0 + 1, 0, 0)
+    t.resize(8 * (size_t)W, 0.0f);
+    float* pairTab = t.data() + 4 * (size_t)W;
+    for (int x0 = 0; x0 + 1 < W; x0 += 2) {
+      const float* c0 = t.data() + 4 * (size_t)x0;
+      const float* c1 = c0 + 4;
+      float* e = pairTab + 4 * (size_t)x0;
+      e[0] = c0[0];
+      e[1] = c1[0];
+      e[2] = c0[1];
+      e[3] = c1[1];
+      e[4] = c0[2];
+      e[5] = c1[2];
+    }
     dev.h2d(xTab, t.data(), t.size() * sizeof(float));
   }
   if (firstAbsorb != absorbX0) {
@@ -395,7 +410,8 @@ int cells3d_create(const Cells3DConfig* cfg, Cells3D** out) {
     h->sdf = (float*)h->dev.alloc((size_t)N * 4, "sdf");
     h->macro = (float4*)h->dev.alloc((size_t)N * 16, "macro");
     h->rowBody = (uint8_t*)h->dev.alloc((size_t)h->H * h->D, "row map");
-    h->xTab = h->dev.alloc((size_t)h->W * 4 * (h->prec == 3 ? 8 : 4), "x table");
+    // f64 rates: 4 per x; f32 rates: 4 per x and the x-pair layout of the same values
+    h->xTab = h->dev.alloc((size_t)h->W * (h->prec == 3 ? 4 * 8 : 8 * 4), "x table");
     h->bodyCells = (int*)h->dev.alloc((size_t)N * 4, "body cell list");
     h->partials = (double4*)h->dev.alloc((size_t)(N / 32 + 2) * sizeof(double4), "force partials");
     h->history = (double4*)h->dev.alloc((size_t)HISTORY_LEN * sizeof(double4), "force history");

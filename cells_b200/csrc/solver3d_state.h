@@ -68,6 +68,11 @@ struct Cells3D : cells::HandleBase {
 
   // the discrete adjoint's recorded forward run (checkpoints, link tables), when one exists
   std::unique_ptr<Adjoint3D> adj;
+  // device memory the adjoint keeps between recorded runs: the checkpoints, the two sets of
+  // recomputed states and the two adjoint states, carved from one block that a later run reuses
+  // while it fits (freed by cells3d_adjoint_release or destroy)
+  void* adjStore = nullptr;
+  size_t adjStoreBytes = 0;
 
   // device scratch of the macro-field products (fields3d.cu), grown on demand
   void* scratch = nullptr;

@@ -452,6 +452,10 @@ template <class C, int ROWS>
 __global__ void __launch_bounds__(256, min_blocks2<C>()) step2d_kernel(const Tunnel2* __restrict__ tunnels,
                                                      const unsigned short* __restrict__ tileTunnel, int par,
                                                      int allowSample) {
+  // programmatic dependent launch, as in the 3D step: the next step's grid is scheduled during
+  // this one's tail and waits here for the previous grid to complete
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const int b = blockIdx.x;
   const int t = __ldg(&tileTunnel[b]);
   tile2<C, ROWS>(tunnels, t, b - __ldg(&tunnels[t].firstTile), par, allowSample);
@@ -515,12 +519,17 @@ __global__ void __launch_bounds__(256, min_blocks2<C>()) step2d_persistent_kerne
 template <class C>
 static cudaError_t launch_step2_t(const Step2Launch& a, cudaStream_t s) {
   if (a.nTiles <= 0) return cudaSuccess;
-  dim3 block(a.tileX, a.tileY);
-  if (a.rows == 2)
-    step2d_kernel<C, 2><<<a.nTiles, block, 0, s>>>(a.tunnels, a.tileTunnel, a.par, a.allowSample);
-  else
-    step2d_kernel<C, 1><<<a.nTiles, block, 0, s>>>(a.tunnels, a.tileTunnel, a.par, a.allowSample);
-  return cudaGetLastError();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(a.nTiles);
+  cfg.blockDim = dim3(a.tileX, a.tileY);
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, a.rows == 2 ? step2d_kernel<C, 2> : step2d_kernel<C, 1>, a.tunnels, a.tileTunnel,
+                            a.par, a.allowSample);
 }
 
 template <class C>

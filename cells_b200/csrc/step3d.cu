@@ -51,6 +51,10 @@ struct StepArgs3 {
   const float* sdf;
   const uint8_t* rowBody;
   const typename Vec4<R>::T* xTab;  // per x: (omega+ without Smagorinsky, omega-, sigma, 0)
+  // per x-pair (x0 = 2j, x0 + 1), for 16-bit storage: entry 2j (omega+ of both, omega- of both),
+  // entry 2j + 1 (sigma of both, 0, 0); the same values as xTab, laid out so a pair's rates load
+  // as register pairs of the packed f32x2 collision
+  const float4* xPair;
   BodyLinks3 links;
   const int* bodyCells;
   double4* partials;
@@ -319,6 +323,177 @@ __device__ __forceinline__ void collide3(const StepArgs3<C>& a, const typename C
   }
 }
 
+
+// ---------------- packed f32x2 arithmetic (sm_100) ----------------
+// One FADD2 / FMUL2 / FFMA2 instruction applies the same f32 operation to two values, each
+// component rounding exactly as the scalar instruction would. The x-pair kernel of 16-bit storage
+// keeps cell x0 in .x and cell x0 + 1 in .y, so one instruction stream updates both cells.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;"
+      : "=l"(d)
+      : "l"(*reinterpret_cast<unsigned long long*>(&a)), "l"(*reinterpret_cast<unsigned long long*>(&b)));
+  return *reinterpret_cast<float2*>(&d);
+}
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+
+// 3 (c_p . u) for the lower member p of each pair, from u3 = 3u
+__device__ __forceinline__ float2 cu3x2(int p, const float2 (&u3)[3]) {
+  switch (p) {
+    case 1: return u3[0];
+    case 3: return u3[1];
+    case 5: return u3[2];
+    case 7: return add2(u3[0], u3[1]);
+    case 9: return add2(u3[0], u3[2]);
+    case 11: return add2(u3[1], u3[2]);
+    case 13: return sub2(u3[0], u3[1]);
+    case 15: return sub2(u3[0], u3[2]);
+    default: return sub2(u3[1], u3[2]);
+  }
+}
+
+// The fast TRT collision of the two cells of an x-pair (cell x0 in .x, x0 + 1 in .y) with packed
+// f32x2 instructions, stored as one 32-bit word per population. It evaluates the lean pair form of
+// collide3 per component in f32: with s_p = f_p + f_p+1 and d_p = f_p - f_p+1 (exact for values
+// of 16-bit storage, whose sums and differences fit the f32 significand),
+//   o_p = S + T, o_p+1 = S - T,  S = (1 - omega+)/2 s_p + omega+ w (rho cu^2/2 + K0),
+//                                T = (1 - omega-)/2 d_p + omega- w rho cu,   K0 = drho - rho usq,
+// which is f_p + A + B and f_p+1 + A - B of collide3 rearranged, so only s_p and d_p stay live.
+// Only the reciprocal of rho, and with Smagorinsky the relaxation time, run per cell.
+// The inlet cell (x0 = 0, when IN) and the outlet cell (x0 + 1 = W - 1, when OUT) go through the
+// same instructions: with omega+ = omega- = 1, rho = 1, drho = 0 and no absorbing source the update
+// is exactly the equilibrium feq(1, u), at u = (uIn, 0, 0) for the inlet (step3d.ts:190-193) and at
+// the node's own velocity for the outlet.
+template <class C, bool SMAG, bool ABS, bool IN, bool OUT>
+__device__ __forceinline__ void collide3x2_store(const StepArgs3<C>& a, const uint32_t (&r)[Q3], int x0, int idx) {
+  constexpr float IS = 1.0f / C::SCALE;
+  float2 sp[Q3], dp[Q3];  // entries p = 1, 3, .., 17
+  const float2 f0 = make_float2(C::lo(r[0]), C::hi(r[0]));
+#pragma unroll
+  for (int p = 1; p < Q3; p += 2) {
+    const float2 fa = make_float2(C::lo(r[p]), C::hi(r[p]));
+    const float2 fb = make_float2(C::lo(r[p + 1]), C::hi(r[p + 1]));
+    sp[p] = add2(fa, fb);
+    dp[p] = sub2(fa, fb);
+  }
+  const float2 dsum = add2(add2(f0, add2(add2(sp[1], sp[3]), add2(sp[5], sp[7]))),
+                           add2(add2(sp[9], sp[11]), add2(sp[13], add2(sp[15], sp[17]))));
+  float2 drho = mul2(dsum, bc2(IS));
+  float2 rho = add2(drho, bc2(1.0f));
+  // the hardware reciprocal (branch-free, within 2 ulp) with 1/SCALE folded in, per cell
+  const float2 invRhoS = make_float2(__fdividef(IS, rho.x), __fdividef(IS, rho.y));
+  float2 ux = mul2(add2(add2(add2(dp[1], dp[7]), add2(dp[9], dp[13])), dp[15]), invRhoS);
+  float2 uy = mul2(add2(add2(add2(dp[3], dp[7]), sub2(dp[11], dp[13])), dp[17]), invRhoS);
+  float2 uz = mul2(sub2(add2(add2(dp[5], dp[9]), sub2(dp[11], dp[15])), dp[17]), invRhoS);
+  const bool inlet = IN && x0 == 0, outlet = OUT && x0 + 1 == a.W - 1;
+  if (inlet) {
+    ux.x = (float)a.st->uIn[a.par];
+    uy.x = 0.0f;
+    uz.x = 0.0f;
+  }
+  const float2 u2 = fma2(uz, uz, fma2(uy, uy, mul2(ux, ux)));
+  const float2 nusq = mul2(bc2(-1.5f), u2);  // -3u^2/2
+  const float2 u3[3] = {mul2(bc2(3.0f), ux), mul2(bc2(3.0f), uy), mul2(bc2(3.0f), uz)};
+  const float4 t0 = a.xPair[x0];
+  float2 omP = make_float2(t0.x, t0.y), omM = make_float2(t0.z, t0.w);
+  if (SMAG) {
+    // second moments of the non-equilibrium part, per pair: n_p + n_p+1 = s_p - 2 w (rho cu^2/2 + K0)
+    const float2 K0s = fma2(rho, nusq, drho);
+    const float2 hr = mul2(bc2(0.5f), rho);
+    float2 pxx, pyy, pzz, pxy, pxz, pyz;
+#pragma unroll
+    for (int p = 1; p < Q3; p += 2) {
+      const float2 cu = cu3x2(p, u3);
+      const float2 n = fma2(bc2(-2.0f * ws3<C>(p)), fma2(mul2(hr, cu), cu, K0s), sp[p]);
+      if (p == 1) pxx = n;
+      else if (cx3(p) != 0) pxx = add2(pxx, n);
+      if (p == 3) pyy = n;
+      else if (cy3(p) != 0) pyy = add2(pyy, n);
+      if (p == 5) pzz = n;
+      else if (cz3(p) != 0) pzz = add2(pzz, n);
+      if (p == 7) pxy = n;
+      else if (cx3(p) * cy3(p) == -1) pxy = sub2(pxy, n);
+      if (p == 9) pxz = n;
+      else if (cx3(p) * cz3(p) == -1) pxz = sub2(pxz, n);
+      if (p == 11) pyz = n;
+      else if (cy3(p) * cz3(p) == -1) pyz = sub2(pyz, n);
+    }
+    const float2 off = fma2(pyz, pyz, fma2(pxz, pxz, mul2(pxy, pxy)));
+    const float2 q = fma2(bc2(2.0f), off, fma2(pzz, pzz, fma2(pyy, pyy, mul2(pxx, pxx))));
+    float om[2], omm[2];
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      const float qc = c ? q.y : q.x, omegaBase = c ? omP.y : omP.x;
+      const float ir = (c ? invRhoS.y : invRhoS.x) * C::SCALE;  // 1/rho, exact: SCALE is a power of two
+      const float pi = sqrtf(qc) * IS;                          // sqrt(SCALE^2 x) = SCALE sqrt(x) exactly
+      const float tt = 1.0f / omegaBase;
+      const float tEff = 0.5f * (tt + sqrtf(tt * tt + 25.45584412271571f * a.smagC2 * pi * ir));
+      om[c] = 1.0f / tEff;
+      omm[c] = 1.0f / (0.5f + a.lambda / (1.0f / om[c] - 0.5f));
+    }
+    omP = make_float2(om[0], om[1]);
+    omM = make_float2(omm[0], omm[1]);
+  }
+  float2 sigma = bc2(0.0f);
+  if (ABS) {
+    const float4 t1 = a.xPair[x0 + 1];
+    sigma = make_float2(t1.x, t1.y);
+  }
+  // the boundary cells relax fully to feq(1, u)
+  if (inlet) {
+    omP.x = omM.x = 1.0f;
+    rho.x = 1.0f;
+    drho.x = 0.0f;
+    sigma.x = 0.0f;
+  }
+  if (outlet) {
+    omP.y = omM.y = 1.0f;
+    rho.y = 1.0f;
+    drho.y = 0.0f;
+    sigma.y = 0.0f;
+  }
+  const bool absorb = ABS && __any_sync(__activemask(), sigma.x > 0.0f || sigma.y > 0.0f);
+  const float2 K0 = fma2(rho, nusq, drho);  // drho - rho usq
+  const float2 aP = fma2(bc2(-0.5f), omP, bc2(0.5f)), aM = fma2(bc2(-0.5f), omM, bc2(0.5f));
+  const float2 hrho = mul2(bc2(0.5f), rho);
+  const float2 cP0 = mul2(omP, bc2(ws3<C>(1))), cP1 = mul2(omP, bc2(ws3<C>(7)));
+  const float2 cPr[2] = {mul2(cP0, hrho), mul2(cP1, hrho)};
+  const float2 cK[2] = {mul2(cP0, K0), mul2(cP1, K0)};
+  const float2 omMr = mul2(omM, rho);
+  const float2 cM[2] = {mul2(omMr, bc2(ws3<C>(1))), mul2(omMr, bc2(ws3<C>(7)))};
+  float2 ut = bc2(0.0f), ndq = bc2(0.0f), sr = bc2(0.0f);
+  if (absorb) {
+    ut = bc2((float)a.st->uIn[a.par]);
+    ndq = mul2(mul2(bc2(-1.5f), rho), fma2(ut, ut, mul2(bc2(-1.0f), u2)));  // -3/2 rho (ut^2 - u^2)
+    sr = mul2(sigma, rho);
+  }
+  {
+    // rest population: (1 - omega+) f0 + omega+ w0 K0
+    float2 v0 = fma2(add2(aP, aP), f0, mul2(omP, mul2(bc2(ws3<C>(0)), K0)));
+    if (absorb) v0 = fma2(mul2(sigma, bc2(ws3<C>(0))), ndq, v0);
+    *reinterpret_cast<uint32_t*>(a.out[0] + idx) = C::pack2_fast(v0.x, v0.y);
+  }
+#pragma unroll
+  for (int p = 1; p < Q3; p += 2) {
+    const int k = p <= 5 ? 0 : 1;
+    const float2 cu = cu3x2(p, u3);
+    float2 S = fma2(aP, sp[p], fma2(mul2(cPr[k], cu), cu, cK[k]));
+    float2 T = fma2(aM, dp[p], mul2(cM[k], cu));
+    if (absorb) {
+      const float2 cut = mul2(bc2(3.0f * (float)cx3(p)), ut);
+      // S += sigma w (rho/2 (cut^2 - cu^2) - dq); T += sigma w rho (cut - cu)
+      const float2 d2 = sub2(mul2(cut, cut), mul2(cu, cu));
+      S = fma2(mul2(sigma, bc2(ws3<C>(p))), fma2(hrho, d2, ndq), S);
+      T = fma2(mul2(sr, bc2(ws3<C>(p))), sub2(cut, cu), T);
+    }
+    const float2 oa = add2(S, T), ob = sub2(S, T);
+    *reinterpret_cast<uint32_t*>(a.out[p] + idx) = C::pack2_fast(oa.x, oa.y);
+    *reinterpret_cast<uint32_t*>(a.out[p + 1] + idx) = C::pack2_fast(ob.x, ob.y);
+  }
+}
 
 template <class C, bool SMAG, bool ABS = true>
 __device__ __forceinline__ void collide_store(const StepArgs3<C>& a, const typename C::R (&f)[Q3], int x, int idx,
@@ -693,6 +868,15 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
     act1 = __ldg(a.flags + idx + 1) == 0u;
     if (!act0 && !act1) return;
   }
+  if constexpr (!kExact) {
+    // fast arithmetic: both cells through the packed f32x2 collision; a pair with one body cell
+    // takes the per-cell code below
+    if (act0 && act1) {
+      // the inlet and outlet tests run per thread (one variant per ABS instead of four)
+      collide3x2_store<C, SMAG, ABS, true, true>(a, r, x0, idx);
+      return;
+    }
+  }
   R o0[Q3];
   if (act0) {
     if (inlet0) {
@@ -727,16 +911,23 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
   }
 }
 
-// Resident blocks per SM the register allocation must allow: 7 for FP16 pairs (72 registers, no
-// spills; measured faster than 6), 6 for BF16 pairs (its half extraction spills at 72).
+// Resident blocks per SM the register allocation must allow: 6 for 16-bit pairs (80 registers;
+// the packed collision measured faster at 6 than at 7, 5 or 4), 8 for f32, 4 for f64.
 template <class C>
 constexpr int step_min_blocks(bool pair) {
-  return pair ? (C::prec == 1 ? 7 : 6) : (sizeof(typename C::R) == 8 ? 4 : 8);
+  return pair ? 6 : (sizeof(typename C::R) == 8 ? 4 : 8);
 }
 
 template <class C, bool SMAG, bool PAIR>
 __global__ void __launch_bounds__(kStepThreads, step_min_blocks<C>(PAIR))
     step3d_kernel(const __grid_constant__ StepArgs3<C> a) {
+  // Programmatic dependent launch: the next step's grid may be scheduled once every block of this
+  // one has started, so its blocks fill the SMs this grid's tail leaves idle; each of them waits
+  // here until the previous grid (launched before it on the stream) has completed and its writes
+  // are visible. Launched without the attribute (or after a non-kernel operation) the wait
+  // returns at once.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   // grid (tilesX, tilesY, roleZ + D - 2): the first roleZ slices of blocks hold the face and body
   // roles (dispatched first), the others the interior tiles, one z plane per slice
   if ((int)blockIdx.z < a.roleZ) {
@@ -795,6 +986,8 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   a.sdf = L.sdf;
   a.rowBody = L.rowBody;
   a.xTab = (const typename Vec4<R>::T*)L.xTab;
+  // the pair layout follows the W per-x entries in the same buffer (f32 rates only)
+  a.xPair = sizeof(R) == 4 ? (const float4*)((const float*)L.xTab + 4 * (size_t)L.W) : nullptr;
   a.bodyCells = L.bodyCells;
   a.links = L.links;
   a.partials = L.partials;
@@ -832,20 +1025,26 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   const dim3 grid(tilesX, tilesY, a.roleZ + zInterior);
   const dim3 block(pair ? L.tileTX / 2 : L.tileTX, kStepThreads / (pair ? L.tileTX / 2 : L.tileTX), 1);
   const bool smag = L.smagC2 > 0;
+  void (*fn)(StepArgs3<C>) = nullptr;
   if (pair) {
-    if constexpr (sizeof(S) == 2) {
-      if (smag)
-        step3d_kernel<C, true, true><<<grid, block, 0, s>>>(a);
-      else
-        step3d_kernel<C, false, true><<<grid, block, 0, s>>>(a);
-    }
+    if constexpr (sizeof(S) == 2) fn = smag ? step3d_kernel<C, true, true> : step3d_kernel<C, false, true>;
   } else {
-    if (smag)
-      step3d_kernel<C, true, false><<<grid, block, 0, s>>>(a);
-    else
-      step3d_kernel<C, false, false><<<grid, block, 0, s>>>(a);
+    fn = smag ? step3d_kernel<C, true, false> : step3d_kernel<C, false, false>;
   }
-  return cudaGetLastError();
+  if (!fn) return cudaErrorInvalidValue;
+  // launched with programmatic stream serialisation: consecutive steps on a stream (and in the
+  // captured step graphs) overlap one grid's launch with the previous grid's tail
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, fn, a);
 }
 
 cudaError_t launch_step3(int precision, const StepLaunch3& a, cudaStream_t s) {

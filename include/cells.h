@@ -250,7 +250,9 @@ typedef struct {
 int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* objective);
 int cells3d_adjoint_backward(Cells3D* h, const void* terminal_adjoint, double* dJ_dsdf, double* dJ_du_in,
                              void* adjoint_out);
-/* Frees the recorded run's checkpoints and tables. */
+/* Frees the recorded run's checkpoints and tables. Without it the device block holding the
+ * checkpoints, the recompute buffers and the adjoint states stays with the handle after a run, and
+ * the next adjoint_forward reuses it while it fits (an optimisation loop allocates it once). */
 int cells3d_adjoint_release(Cells3D* h);
 
 /* ---------------- state save / restore (no counterpart in the reference) ----------------

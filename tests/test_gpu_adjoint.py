@@ -149,8 +149,15 @@ def test_star_drag_config_gradient_and_cost():
     ref = np.array([fd[k] for k in range(17)])
     scale = np.max(np.abs(ref))
     err = np.max(np.abs(adj - ref)) / scale
+    rel = np.abs(adj - ref) / np.maximum(np.abs(ref), 1e-300)
     print(f"J {J:.6f}  cost backward/forward {t_bwd / t_fwd:.2f}  max error {err:.2e} of |grad|max {scale:.3e}"
           f"  flips {flips}")
+    print("per component: fd", np.array2string(ref, precision=5), "relative error", np.array2string(rel, precision=2))
     assert all(v == 0 for v in flips.values()), flips
     assert err <= 1e-3, (adj, ref)
+    # 1e-3 relative on every component above the floor of 0.1 max|FD|; below it the FP32 run's own
+    # rounding (about 1e-5 of the largest component) is a larger share than 1e-3 of the value
+    big = np.abs(ref) >= 0.1 * scale
+    assert big.sum() >= 3, ref
+    assert np.all(rel[big] <= 1e-3), (rel, ref)
     assert t_bwd <= 4.0 * t_fwd, (t_bwd, t_fwd)

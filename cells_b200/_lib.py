@@ -112,6 +112,7 @@ def lib() -> C.CDLL:
         "cells3d_init_field": (I, [P, P]),
         "cells3d_reset_forces": (I, [P]),
         "cells3d_step": (I, [P, I64]),
+        "cells3d_prepare_steps": (I, [P, I64]),
         "cells3d_update_macro": (I, [P]),
         "cells3d_run": (I, [P, I64, I64]),
         "cells3d_synchronize": (I, [P]),

@@ -298,6 +298,21 @@ void Cells3D::launch_steps(int64_t n) {
   }
 }
 
+// Builds (captures and instantiates) every step graph that launch_steps(n) from the current step
+// would replay, without running anything, so a timed or latency-critical run that follows replays
+// graphs only.
+void Cells3D::prepare_steps(int64_t n) {
+  const int period = graph_period();
+  if (dev.fake || !useGraphs || period > kMaxGraphPeriod) return;
+  int64_t s = step;
+  while (n >= kGraphSteps) {
+    const int phase = (int)(s % period);
+    if (!graphs[phase].exec || graphs[phase].gen != argGen) build_graph(phase);
+    s += kGraphSteps;
+    n -= kGraphSteps;
+  }
+}
+
 void Cells3D::free_all() {
   adj.reset();  // its buffers are the device's; freed by dev.close below
   for (auto& g : graphs)
@@ -562,6 +577,14 @@ int cells3d_step(Cells3D* h, int64_t n) {
   CELLS_TRY(h)
   if (n < 0) throw Error(CELLS_E_INVALID, "negative step count");
   h->launch_steps(n);
+  CELLS_CATCH(h)
+}
+
+int cells3d_prepare_steps(Cells3D* h, int64_t n) {
+  if (!h) return CELLS_E_INVALID;
+  CELLS_TRY(h)
+  if (n < 0) throw Error(CELLS_E_INVALID, "negative step count");
+  h->prepare_steps(n);
   CELLS_CATCH(h)
 }
 

@@ -121,6 +121,7 @@ struct Cells3D : cells::HandleBase {
   int graph_period() const;
   void build_graph(int phase);
   void launch_steps(int64_t n);
+  void prepare_steps(int64_t n);
   void write_state(int which);
   void free_all();
 };

@@ -126,6 +126,11 @@ class Solver3D:
     def encodeSteps(self, n: int) -> None:
         check(lib().cells3d_step(self._h, n), self._h)
 
+    def prepareSteps(self, n: int) -> None:
+        """Builds the CUDA graphs that encodeSteps(n) from the current step would replay, running
+        nothing (no counterpart in the reference)."""
+        check(lib().cells3d_prepare_steps(self._h, n), self._h)
+
     def encodeMacro(self) -> None:
         check(lib().cells3d_update_macro(self._h), self._h)
 

@@ -139,6 +139,10 @@ int cells3d_reset_forces(Cells3D* h);                       /* resetForces */
 /* ---------------- stepping ---------------- */
 /* encodeSteps (src/solver3d.ts:252-267): enqueue n steps; returns without waiting. */
 int cells3d_step(Cells3D* h, int64_t n);
+/* No counterpart in the reference: builds the CUDA graphs that cells3d_step(h, n) from the current
+ * step would replay (128 steps each), without running anything, so that a timed or latency-critical
+ * run replays graphs only. A later parameter, SDF or ramp change invalidates them. */
+int cells3d_prepare_steps(Cells3D* h, int64_t n);
 /* encodeMacro (src/solver3d.ts:269-273): refresh the macro buffer from the latest populations. */
 int cells3d_update_macro(Cells3D* h);
 /* run (src/solver3d.ts:276-288): n steps, then the macro refresh, then wait for the GPU. The

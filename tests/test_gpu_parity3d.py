@@ -400,3 +400,21 @@ def test_config2_fp16_fast_against_oracle():
     print("velocity L2", l2)
     assert l2 <= 1e-3
     s.destroy()
+
+
+def test_prepare_steps_runs_nothing_and_graphs_match():
+    """prepareSteps captures the step graphs ahead of a run without stepping: the state is unchanged
+    and the prepared run matches the oracle bit for bit."""
+    W, H, D = 20, 10, 8
+    s, o = pair(W, H, D, "fp32", True, sphere_sdf(W, H, D, 6, 5, 4, 2), forceEvery=2)
+    s.encodeSteps(3)
+    o.encodeSteps(3)
+    before = s.readPopulations().copy()
+    s.prepareSteps(300)
+    assert s.step == 3
+    assert np.array_equal(s.readPopulations().view(np.uint32), before.view(np.uint32))
+    s.encodeSteps(300)
+    o.encodeSteps(300)
+    assert_same(s, o, True)
+    assert_forces(s.readForces(), o.readForces(), 1e-9)
+    s.destroy()

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "adjoint3d.h"
@@ -380,17 +381,33 @@ cudaError_t launch_adjoint_step3(int precision, const AdjLaunch3& a, cudaStream_
 
 namespace {
 
+// Host threads for the table builds: the machine's, at most 16.
+int table_threads() {
+  const unsigned n = std::thread::hardware_concurrency();
+  return (int)std::max(1u, std::min(16u, n));
+}
+
+// Runs fn(t) for t = 0 .. n-1 on n host threads (t = 0 on the caller's).
+template <class F>
+void run_threads(int n, F fn) {
+  std::vector<std::thread> pool;
+  for (int t = 1; t < n; t++) pool.emplace_back(fn, t);
+  fn(0);
+  for (std::thread& th : pool) th.join();
+}
+
+// The links of the flagged fluid cells of planes z0 .. z1-1, in cell order; base[idx] is set to the
+// first link of each such cell, counted within this slab's links.
 template <class R>
-void resolve_links(const Cells3D* h, const std::vector<uint32_t>& fl, const std::vector<float>& sdf, int comp,
-                   std::vector<int>& base, std::vector<AdjLink3Host>& links) {
+void resolve_links_slab(const Cells3D* h, const std::vector<uint32_t>& fl, const std::vector<float>& sdf, int comp,
+                        int z0, int z1, std::vector<int>& base, std::vector<AdjLink3Host>& links) {
   const int W = h->W, H = h->H, D = h->D;
   const long long N = h->N;
   auto at = [&](int x, int y, int z) { return (long long)x + (long long)W * ((long long)y + (long long)H * z); };
   auto solid = [&](long long c) { return (fl[(size_t)c] & FLAG3_SOLID) != 0u; };
   auto cc = [&](int j) { return comp == 0 ? cx3(j) : (comp == 1 ? cy3(j) : cz3(j)); };
-  base.assign((size_t)N, -1);
   links.clear();
-  for (int z = 0; z < D; z++)
+  for (int z = z0; z < z1; z++)
     for (int y = 0; y < H; y++)
       for (int x = 0; x < W; x++) {
         const long long idx = at(x, y, z);
@@ -475,6 +492,31 @@ void resolve_links(const Cells3D* h, const std::vector<uint32_t>& fl, const std:
       }
 }
 
+// The link records of every flagged fluid cell in cell order (the order a sequential pass gives),
+// built by slabs of planes on host threads and joined.
+template <class R>
+void resolve_links(const Cells3D* h, const std::vector<uint32_t>& fl, const std::vector<float>& sdf, int comp,
+                   std::vector<int>& base, std::vector<AdjLink3Host>& links) {
+  const int D = h->D;
+  const long long plane = (long long)h->W * h->H;
+  base.assign((size_t)h->N, -1);
+  const int T = std::min(table_threads(), D);
+  std::vector<std::vector<AdjLink3Host>> part((size_t)T);
+  auto z_begin = [&](int t) { return (int)((long long)D * t / T); };
+  run_threads(T, [&](int t) { resolve_links_slab<R>(h, fl, sdf, comp, z_begin(t), z_begin(t + 1), base, part[(size_t)t]); });
+  std::vector<int> offset((size_t)T + 1, 0);
+  for (int t = 0; t < T; t++) offset[(size_t)t + 1] = offset[(size_t)t] + (int)part[(size_t)t].size();
+  run_threads(T, [&](int t) {
+    const int o = offset[(size_t)t];
+    if (o == 0) return;
+    for (long long c = z_begin(t) * plane; c < z_begin(t + 1) * plane; c++)
+      if (base[(size_t)c] >= 0) base[(size_t)c] += o;
+  });
+  links.clear();
+  links.reserve((size_t)offset[(size_t)T]);
+  for (auto& p : part) links.insert(links.end(), p.begin(), p.end());
+}
+
 template <class R>
 void upload_typed(cells::Device& dev, void* d, const std::vector<double>& v) {
   std::vector<R> t(v.begin(), v.end());
@@ -549,24 +591,33 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
   std::sort(key.begin(), key.end());
   // elements without a regular reader, generated in increasing element order (direction outer)
   auto at = [&](int x, int y, int z) { return (long long)x + (long long)W * ((long long)y + (long long)H * z); };
-  std::vector<long long> irregular;
-  for (int i = 0; i < Q3; i++)
-    for (int z = 0; z < D; z++)
-      for (int y = 0; y < H; y++) {
-        const int ry = y + cy3(i), rz = z + cz3(i);
-        const bool rowIn = ry >= 0 && ry < H && rz >= 0 && rz < D;
-        for (int x = 0; x < W; x++) {
-          const long long c = at(x, y, z);
-          if (fl[(size_t)c] & FLAG3_SOLID) continue;
-          const int rx = x + cx3(i);
-          bool regular = rowIn && rx >= 0 && rx < W;
-          if (regular) {
-            const uint32_t g = fl[(size_t)at(rx, ry, rz)];
-            regular = !(g & (FLAG3_SOLID | FLAG3_INLET)) && (i == 0 || !(g & (1u << i)));
+  std::vector<std::vector<long long>> irr(Q3);  // per direction, on host threads
+  {
+    const int T = std::min(table_threads(), Q3);
+    run_threads(T, [&](int t) {
+      for (int i = t; i < Q3; i += T) {
+        std::vector<long long>& out = irr[(size_t)i];
+        for (int z = 0; z < D; z++)
+          for (int y = 0; y < H; y++) {
+            const int ry = y + cy3(i), rz = z + cz3(i);
+            const bool rowIn = ry >= 0 && ry < H && rz >= 0 && rz < D;
+            for (int x = 0; x < W; x++) {
+              const long long c = at(x, y, z);
+              if (fl[(size_t)c] & FLAG3_SOLID) continue;
+              const int rx = x + cx3(i);
+              bool regular = rowIn && rx >= 0 && rx < W;
+              if (regular) {
+                const uint32_t g = fl[(size_t)at(rx, ry, rz)];
+                regular = !(g & (FLAG3_SOLID | FLAG3_INLET)) && (i == 0 || !(g & (1u << i)));
+              }
+              if (!regular) out.push_back(i * N + c);
+            }
           }
-          if (!regular) irregular.push_back(i * N + c);
-        }
       }
+    });
+  }
+  std::vector<long long> irregular;
+  for (auto& v : irr) irregular.insert(irregular.end(), v.begin(), v.end());
   // merge: for one element the link entries come before its no-reader mark
   std::vector<Ent> ents;
   ents.reserve(lent.size() + irregular.size());

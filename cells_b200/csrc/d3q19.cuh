@@ -70,6 +70,16 @@ struct CodecF32 {
   __device__ __forceinline__ static S enc(R v) { return v; }
   __device__ __forceinline__ static R raw(const S* p) { return __ldg(p); }
   __device__ __forceinline__ static S enc_raw(R v) { return v; }
+  // x-pairs (cells x0, x0 + 1, x0 even): one 8-byte word, or two 4-byte loads for a shifted pair
+  using Pair = float2;
+  __device__ __forceinline__ static Pair ld_pair(const S* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+  __device__ __forceinline__ static Pair ld_pair2(const S* p0, const S* p1) {
+    return make_float2(__ldg(p0), __ldg(p1));
+  }
+  __device__ __forceinline__ static R lo(Pair w) { return w.x; }
+  __device__ __forceinline__ static R hi(Pair w) { return w.y; }
+  __device__ __forceinline__ static void st_pair(S* p, R a, R b) { *reinterpret_cast<float2*>(p) = make_float2(a, b); }
+  __device__ __forceinline__ static void st_pair_fast(S* p, R a, R b) { st_pair(p, a, b); }
 };
 struct CodecF16 {
   using S = __half;
@@ -104,6 +114,14 @@ struct CodecF16 {
     asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(b), "f"(a));
     return d;
   }
+  using Pair = uint32_t;
+  __device__ __forceinline__ static Pair ld_pair(const S* p) { return __ldg(reinterpret_cast<const unsigned int*>(p)); }
+  __device__ __forceinline__ static Pair ld_pair2(const S* p0, const S* p1) {
+    return (uint32_t)__ldg(reinterpret_cast<const unsigned short*>(p0)) |
+           ((uint32_t)__ldg(reinterpret_cast<const unsigned short*>(p1)) << 16);
+  }
+  __device__ __forceinline__ static void st_pair(S* p, R a, R b) { *reinterpret_cast<uint32_t*>(p) = pack2(a, b); }
+  __device__ __forceinline__ static void st_pair_fast(S* p, R a, R b) { *reinterpret_cast<uint32_t*>(p) = pack2_fast(a, b); }
 };
 struct CodecBF16 {
   using S = __nv_bfloat16;
@@ -121,6 +139,14 @@ struct CodecBF16 {
     return *reinterpret_cast<uint32_t*>(&h);
   }
   __device__ __forceinline__ static uint32_t pack2_fast(R a, R b) { return pack2(a, b); }
+  using Pair = uint32_t;
+  __device__ __forceinline__ static Pair ld_pair(const S* p) { return __ldg(reinterpret_cast<const unsigned int*>(p)); }
+  __device__ __forceinline__ static Pair ld_pair2(const S* p0, const S* p1) {
+    return (uint32_t)__ldg(reinterpret_cast<const unsigned short*>(p0)) |
+           ((uint32_t)__ldg(reinterpret_cast<const unsigned short*>(p1)) << 16);
+  }
+  __device__ __forceinline__ static void st_pair(S* p, R a, R b) { *reinterpret_cast<uint32_t*>(p) = pack2(a, b); }
+  __device__ __forceinline__ static void st_pair_fast(S* p, R a, R b) { *reinterpret_cast<uint32_t*>(p) = pack2_fast(a, b); }
 };
 struct CodecF64 {
   using S = double;

@@ -55,12 +55,13 @@ static void fill_xtab(std::vector<R>& t, int W, double tau, double lambda, doubl
 }
 
 // Interior tile of the step kernel (128 threads per block): 128 cells, or 256 cells as x-pairs for
-// 16-bit storage with an even width. The tile width is workgroup_size when given (the autotuner's
-// knob), else the candidate that wastes the fewest threads at the end of a row: the widest for one
-// cell per thread, the narrowest (64 cells, 32 pairs x 4 rows) for pairs, whose issue-bound kernel
-// gains when more tiles fall wholly outside the absorbing layer and the outlet column.
+// f32, f16 or bf16 storage with an even width (f64 and odd widths take one cell per thread). The
+// tile width is workgroup_size when given (the autotuner's knob), else the candidate that wastes
+// the fewest threads at the end of a row: the widest for one cell per thread, the narrowest (64
+// cells, 32 pairs x 4 rows) for pairs, so that more tiles fall wholly outside the absorbing layer
+// and the outlet column.
 void Cells3D::choose_launch() {
-  pairTiles = (bpp == 2 && (W % 2) == 0) ? 1 : 0;
+  pairTiles = (bpp <= 4 && (W % 2) == 0) ? 1 : 0;
   const int cells = pairTiles ? 256 : 128;
   const int lo = pairTiles ? 64 : 32;
   int best = -1;

@@ -326,8 +326,8 @@ __device__ __forceinline__ void collide3(const StepArgs3<C>& a, const typename C
 
 // ---------------- packed f32x2 arithmetic (sm_100) ----------------
 // One FADD2 / FMUL2 / FFMA2 instruction applies the same f32 operation to two values, each
-// component rounding exactly as the scalar instruction would. The x-pair kernel of 16-bit storage
-// keeps cell x0 in .x and cell x0 + 1 in .y, so one instruction stream updates both cells.
+// component rounding exactly as the scalar instruction would. The x-pair kernel keeps cell x0 in .x
+// and cell x0 + 1 in .y, so one instruction stream updates both cells.
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
@@ -358,7 +358,7 @@ __device__ __forceinline__ float2 cu3x2(int p, const float2 (&u3)[3]) {
 // The fast TRT collision of the two cells of an x-pair (cell x0 in .x, x0 + 1 in .y) with packed
 // f32x2 instructions, stored as one 32-bit word per population. It evaluates the lean pair form of
 // collide3 per component in f32: with s_p = f_p + f_p+1 and d_p = f_p - f_p+1 (exact for values
-// of 16-bit storage, whose sums and differences fit the f32 significand),
+// of 16-bit storage, whose sums and differences fit the f32 significand; rounded once for f32),
 //   o_p = S + T, o_p+1 = S - T,  S = (1 - omega+)/2 s_p + omega+ w (rho cu^2/2 + K0),
 //                                T = (1 - omega-)/2 d_p + omega- w rho cu,   K0 = drho - rho usq,
 // which is f_p + A + B and f_p+1 + A - B of collide3 rearranged, so only s_p and d_p stay live.
@@ -368,7 +368,8 @@ __device__ __forceinline__ float2 cu3x2(int p, const float2 (&u3)[3]) {
 // is exactly the equilibrium feq(1, u), at u = (uIn, 0, 0) for the inlet (step3d.ts:190-193) and at
 // the node's own velocity for the outlet.
 template <class C, bool SMAG, bool ABS, bool IN, bool OUT>
-__device__ __forceinline__ void collide3x2_store(const StepArgs3<C>& a, const uint32_t (&r)[Q3], int x0, int idx) {
+__device__ __forceinline__ void collide3x2_store(const StepArgs3<C>& a, const typename C::Pair (&r)[Q3], int x0,
+                                                 int idx) {
   constexpr float IS = 1.0f / C::SCALE;
   float2 sp[Q3], dp[Q3];  // entries p = 1, 3, .., 17
   const float2 f0 = make_float2(C::lo(r[0]), C::hi(r[0]));
@@ -474,7 +475,7 @@ __device__ __forceinline__ void collide3x2_store(const StepArgs3<C>& a, const ui
     // rest population: (1 - omega+) f0 + omega+ w0 K0
     float2 v0 = fma2(add2(aP, aP), f0, mul2(omP, mul2(bc2(ws3<C>(0)), K0)));
     if (absorb) v0 = fma2(mul2(sigma, bc2(ws3<C>(0))), ndq, v0);
-    *reinterpret_cast<uint32_t*>(a.out[0] + idx) = C::pack2_fast(v0.x, v0.y);
+    C::st_pair_fast(a.out[0] + idx, v0.x, v0.y);
   }
 #pragma unroll
   for (int p = 1; p < Q3; p += 2) {
@@ -490,8 +491,8 @@ __device__ __forceinline__ void collide3x2_store(const StepArgs3<C>& a, const ui
       T = fma2(mul2(sr, bc2(ws3<C>(p))), sub2(cut, cu), T);
     }
     const float2 oa = add2(S, T), ob = sub2(S, T);
-    *reinterpret_cast<uint32_t*>(a.out[p] + idx) = C::pack2_fast(oa.x, oa.y);
-    *reinterpret_cast<uint32_t*>(a.out[p + 1] + idx) = C::pack2_fast(ob.x, ob.y);
+    C::st_pair_fast(a.out[p] + idx, oa.x, oa.y);
+    C::st_pair_fast(a.out[p + 1] + idx, ob.x, ob.y);
   }
 }
 
@@ -826,11 +827,12 @@ __device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int tz) {
   collide_store<C, SMAG, ABS>(a, f, x, idx, outlet);
 }
 
-// Interior rows for 16-bit storage (f16, bf16) and an even width: each thread updates the x-pair
+// Interior rows for f32, f16 and bf16 storage and an even width: each thread updates the x-pair
 // (x0, x0 + 1), x0 even. One address per population serves both cells; the populations with c_x = 0
-// arrive as one 32-bit load (both cells' values), the others as two 16-bit loads; the 19 results are
-// rounded as a pair and stored with one 32-bit store. Cells of the pair that belong to the body role
-// are left alone. ABS / OUT: the tile overlaps the absorbing layer / holds the outlet column.
+// arrive as one word holding both cells' values (8 bytes for f32, 4 for 16-bit storage), the
+// others as two single-cell loads; the 19 results are stored as one word per population. Cells of
+// the pair that belong to the body role are left alone. ABS / OUT: the tile overlaps the absorbing
+// layer / holds the outlet column.
 template <class C, bool SMAG, bool ABS, bool OUT>
 __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
   using R = typename C::R;
@@ -847,19 +849,17 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
   const long long WH = (long long)W * H;
   // the pulls go out before the body-row test, so they do not wait for it (every interior pull
   // address is inside the grid; a pair of body cells discards them)
-  uint32_t r[Q3];  // populations of the pair: x0 in the low half, x0 + 1 in the high half
+  typename C::Pair r[Q3];  // populations of the pair: x0 in the low half (.x), x0 + 1 in the high half
 #pragma unroll
   for (int i = 0; i < Q3; i++) {
     const S* p = a.pull[i] + idx;
     if (cx3(i) == 0) {
-      r[i] = __ldg(reinterpret_cast<const unsigned int*>(p));
+      r[i] = C::ld_pair(p);
     } else {
       int e1 = 1;
       // outlet: zero-gradient copy from (W-2, y, z) for the directions entering through x = W-1
       if (cx3(i) == -1 && outlet1) e1 += (int)(-2 + cy3(i) * (long long)W + cz3(i) * WH);
-      const uint32_t v0 = __ldg(reinterpret_cast<const unsigned short*>(p));
-      const uint32_t v1 = __ldg(reinterpret_cast<const unsigned short*>(p + e1));
-      r[i] = v0 | (v1 << 16);
+      r[i] = C::ld_pair2(p, p + e1);
     }
   }
   bool act0 = true, act1 = true;
@@ -901,7 +901,7 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
   if (act0 && act1) {
 #pragma unroll
     for (int i = 0; i < Q3; i++)
-      *reinterpret_cast<uint32_t*>(a.out[i] + idx) = kExact ? C::pack2(o0[i], o1[i]) : C::pack2_fast(o0[i], o1[i]);
+      kExact ? C::st_pair(a.out[i] + idx, o0[i], o1[i]) : C::st_pair_fast(a.out[i] + idx, o0[i], o1[i]);
   } else if (act0) {
 #pragma unroll
     for (int i = 0; i < Q3; i++) a.out[i][idx] = C::enc_raw(o0[i]);
@@ -911,8 +911,9 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
   }
 }
 
-// Resident blocks per SM the register allocation must allow: 6 for 16-bit pairs (80 registers;
-// the packed collision measured faster at 6 than at 7, 5 or 4), 8 for f32, 4 for f64.
+// Resident blocks per SM the register allocation must allow: 6 for x-pairs (80 registers; the
+// packed collision measured faster at 6 than at 7, 5 or 4), 8 for one f32 cell per thread (odd
+// widths), 4 for f64.
 template <class C>
 constexpr int step_min_blocks(bool pair) {
   return pair ? 6 : (sizeof(typename C::R) == 8 ? 4 : 8);
@@ -1013,7 +1014,7 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   // the body role runs when there are body cells, and on sampled steps even without them (a
   // sample of zero force is still written to the ring, as the reference's reduce pass does)
   a.bodyBlocks = (L.nBody > 0 || L.sample) ? body_blocks3(L.nBody) : 0;
-  const bool pair = sizeof(S) == 2 && (L.W % 2) == 0 && L.tileTX >= 64 && L.pairTiles;
+  const bool pair = sizeof(S) <= 4 && (L.W % 2) == 0 && L.tileTX >= 64 && L.pairTiles;
   if (!pair && L.tileTX > kStepThreads) return cudaErrorInvalidValue;
   a.tileTX = L.tileTX;
   a.tileTY = L.tileTY;
@@ -1027,7 +1028,7 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   const bool smag = L.smagC2 > 0;
   void (*fn)(StepArgs3<C>) = nullptr;
   if (pair) {
-    if constexpr (sizeof(S) == 2) fn = smag ? step3d_kernel<C, true, true> : step3d_kernel<C, false, true>;
+    if constexpr (sizeof(S) <= 4) fn = smag ? step3d_kernel<C, true, true> : step3d_kernel<C, false, true>;
   } else {
     fn = smag ? step3d_kernel<C, true, false> : step3d_kernel<C, false, false>;
   }

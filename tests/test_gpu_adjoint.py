@@ -111,24 +111,25 @@ def link_classes(sdf, W, H, D):
     return out
 
 
-def flip_free_coef(problem, first_stream, h=1e-4):
+def flip_free_coef(problem, first_stream, h=1e-4, kinks=True):
     """The first seeded draw c ~ N(0, 0.02^2) (streams first_stream, first_stream + 1, ...) for which
     no node changes solidity and no Bouzidi link changes the piece of its q(sdf) under c_k +- h for
     any k: a flip is a discrete change of the geometry, and a link crossing q = 1/2 or a clamp is a
-    kink of J, where a central difference is not the derivative."""
+    kink of J, where a central difference is not the derivative. kinks=False checks solidity only
+    (for bodies with thousands of links some link always lies within h of a kink)."""
     dims = (problem.W, problem.H, problem.D)
     for stream in range(first_stream, first_stream + 50):
         coef = 0.02 * normal(SEED, stream, 16)
         s0 = problem.sdf(coef)
         base = s0 < 0
-        cls0 = link_classes(s0, *dims)
+        cls0 = link_classes(s0, *dims) if kinks else None
         ok = True
         for k in range(16):
             for sgn in (1, -1):
                 c = coef.copy()
                 c[k] += sgn * h
                 s1 = problem.sdf(c)
-                if np.any((s1 < 0) != base) or np.any(link_classes(s1, *dims) != cls0):
+                if np.any((s1 < 0) != base) or (kinks and np.any(link_classes(s1, *dims) != cls0)):
                     ok = False
                     break
             if not ok:
@@ -159,7 +160,7 @@ def test_star_gradient_matches_central_differences_fp64():
 def test_star_drag_config_gradient_and_cost():
     """128x64x64, Re 150, 6000 steps, C_D over labels 4000..6000, K = 100: FP32 adjoint vs FP64 FD."""
     p = StarDrag(precision="fp32")
-    coef = flip_free_coef(p, 5)
+    coef = flip_free_coef(p, 5, kinks=False)
     J = p.forward(coef)
     p.solver.synchronize()
     # the cost compared is the adjoint sweep (recompute included); the chain rule to the 16

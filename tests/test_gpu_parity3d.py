@@ -116,10 +116,10 @@ def test_smagorinsky_fixed_lambda_cylinder_touching_slip_faces(precision):
     s.destroy()
 
 
-@pytest.mark.parametrize("precision", ["fp16", "bf16"])
-def test_odd_width_16bit_exact(precision):
-    """An odd width: 16-bit storage takes the one-cell-per-thread interior kernel (16-bit loads)
-    instead of x-pairs, with the per-side face rows."""
+@pytest.mark.parametrize("precision", ["fp16", "bf16", "fp32"])
+def test_odd_width_exact(precision):
+    """An odd width: the one-cell-per-thread interior kernel instead of x-pairs (16-bit loads and
+    the per-side face rows for 16-bit storage)."""
     W, H, D = 23, 14, 10
     s, o = pair(W, H, D, precision, True, sphere_sdf(W, H, D, 8, 7, 5, 3))
     for n in (1, 20):
@@ -127,6 +127,18 @@ def test_odd_width_16bit_exact(precision):
         o.encodeSteps(n)
         assert_same(s, o, True)
     assert_forces(s.readForces(), o.readForces(), 1e-9)
+    s.destroy()
+
+
+def test_odd_width_fast_fp32():
+    """The one-cell-per-thread kernel in fast arithmetic (odd width): within 2e-6 of the oracle."""
+    W, H, D = 23, 14, 10
+    s, o = pair(W, H, D, "fp32", False, sphere_sdf(W, H, D, 8, 7, 5, 3))
+    for n in (1, 29):
+        s.encodeSteps(n)
+        o.encodeSteps(n)
+        assert_same(s, o, False, 2e-6)
+    assert_forces(s.readForces(), o.readForces(), 1e-5)
     s.destroy()
 
 
@@ -278,11 +290,11 @@ def test_state_snapshot_resumes_bit_for_bit():
 #
 # The interior kernel is chosen per block from the tile's x range: tiles that end before the first
 # absorbing column compile without the absorbing sources (ABS = false), tiles that do not hold the
-# outlet column without its rules (OUT = false). At W = 200 the FP32 / FP64 kernels take 7 tiles of
-# 32 cells (tiles 0-4 ABS = OUT = false, tile 5 ABS only, tile 6 both) and the 16-bit x-pair kernel
-# 4 tiles of 64 cells (tiles 0-1 neither, tile 2 ABS only, tile 3 both). With absorb = 0 every tile
-# has ABS = false and the last one OUT = true. The bodies sit in tiles of each kind, so body rows
-# (the flag test of the pair kernel) occur in each too.
+# outlet column without its rules (OUT = false). At W = 200 the FP64 kernel takes 7 tiles of 32
+# cells (tiles 0-4 ABS = OUT = false, tile 5 ABS only, tile 6 both) and the x-pair kernel of FP32
+# and 16-bit storage 4 tiles of 64 cells (tiles 0-1 neither, tile 2 ABS only, tile 3 both). With
+# absorb = 0 every tile has ABS = false and the last one OUT = true. The bodies sit in tiles of each
+# kind, so body rows (the flag test of the pair kernel) occur in each too.
 
 WIDE = (200, 12, 10)
 
@@ -290,9 +302,9 @@ WIDE = (200, 12, 10)
 def wide_sdf():
     W, H, D = WIDE
     sdf = g.empty_sdf3(W, H, D)
-    g.add_sphere(sdf, W, H, D, 41, 6, 5, 3)      # FP32 tile 1, pair tile 0
-    g.add_sphere(sdf, W, H, D, 99.5, 5, 4, 2.5)  # FP32 tile 3, pair tile 1, across two x tiles
-    g.add_box3(sdf, W, H, D, 178, 7, 5, 2, 2, 2)  # FP32 tile 5, pair tile 2: inside the absorbing layer
+    g.add_sphere(sdf, W, H, D, 41, 6, 5, 3)      # FP64 tile 1, pair tile 0
+    g.add_sphere(sdf, W, H, D, 99.5, 5, 4, 2.5)  # FP64 tile 3, pair tile 1, across two x tiles
+    g.add_box3(sdf, W, H, D, 178, 7, 5, 2, 2, 2)  # FP64 tile 5, pair tile 2: inside the absorbing layer
     return sdf
 
 
@@ -302,7 +314,7 @@ def test_multi_tile_exact(precision, absorb):
     W, H, D = WIDE
     s, o = pair(W, H, D, precision, True, wide_sdf(), absorb=absorb)
     info = s.info()
-    tile = 64 if precision in ("fp16", "bf16") else 32
+    tile = 32 if precision == "fp64" else 64  # x-pair tiles for f32 and 16-bit storage
     assert info["block_x"] == tile, info  # tile width in cells
     assert np.array_equal(s.readFlags(), o.flags)
     for n in (1, 4, 20):

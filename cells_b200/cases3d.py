@@ -4,6 +4,11 @@
   Re 100 on 192x96x96, FP32 and FP16 storage each run in blocks of 2000 steps (smoothstep inlet ramp
   over 3000 steps set per chunk of 400, forces every 4 steps) until C_D changes by less than 1e-4
   between blocks; gate: C_D of FP16 within 1% of FP32. BF16 and FP64 are added beside them.
+* ``sphere_wake``: the 3D page's sphere (size fraction 0.2 of the height, 19.2 cells, at (W/4, H/2,
+  D/2) of 192x96x96; u = 0.1 smoothstep-ramped over 3000 steps; sponge 0.15, absorb 0.02; forces
+  every 4 steps; from rest, src/app3d.ts:18-20,182,314-315, src/tunnel3d.ts:38-72) at a given Re,
+  for the wake regimes the reference reports (README.md:73): at Re 250 a steady wake that leans to
+  one side (C_L 0.063), at Re 300 shedding with St 0.135.
 * ``precision_sweep``: four obstacles (sphere D=20, cube edge 18, spanwise cylinder D=16, NACA0012
   wing chord 40 over the full span at 6 degrees) at Re 200 on 256x128x128, stored as FP32, FP16
   and BF16 with FP32 arithmetic, 4000 steps; time-averaged C_D and C_L over steps 2000..4000 and the
@@ -151,3 +156,39 @@ def sweep_table(rows) -> str:
                        f"| {e['C_L_abs_err_vs_fp64']:.2e} | {e['C_D_err_vs_fp64_half_grid']:.2e} "
                        f"| {e['vel_L2_vs_fp64']:.2e} |")
     return "\n".join(out)
+
+
+def sphere_wake(re: float, steps: int = 40000, precision: str = "fp32", device: int = 0, grid=(192, 96, 96)) -> dict:
+    """The 3D page's sphere at Reynolds number re (module docstring). Returns the side-force
+    coefficients C_y and C_z averaged over the second half of the run (the page's C_L readout is
+    C_y over the second half of its force history), their magnitude, C_D over the same half, and the
+    Strouhal number of the side force with the larger oscillation over the last 15,000 steps."""
+    W, H, D = grid
+    body = analysis.build_body("sphere", 0.2, 0.0, W, H, D)
+    L, u = body["lRef"], 0.1
+    tau = derive_tau(re, u, L).tau
+    s = Solver3D.create(W, H, D, precision=precision, tau=tau, uIn=0.0, spongeFraction=0.15, spongeTau=1.0,
+                        absorb=0.02, forceEvery=4, device=device)
+    s.setSdf(body["sdf"])
+    s.initField()
+    s.setInletRamp("smoothstep", u, 3000, 1)
+    chunks = []
+    done = 0
+    while done < steps:
+        k = min(20000, steps - done)  # the ring holds 8192 samples, 32,768 steps at every 4th
+        s.encodeSteps(k)
+        done += k
+        chunks.append(s.readForcesArray())
+    s.destroy()
+    f = np.concatenate(chunks)
+    scale = 2 / (u * u * body["area"])
+    half = f[f[:, 0] > steps / 2]
+    cy, cz = scale * float(np.mean(half[:, 2])), scale * float(np.mean(half[:, 3]))
+    tail = f[f[:, 0] > steps - 15000]
+    comp = 2 if np.ptp(tail[:, 2]) >= np.ptp(tail[:, 3]) else 3
+    p = analysis.period_from_crossings(list(tail[:, 0]), list(tail[:, comp]))
+    st = L / (p[0] * u) if p else math.nan
+    return {"re": re, "tau": tau, "steps": steps, "precision": precision, "L": L,
+            "C_D": scale * float(np.mean(half[:, 1])), "C_y": cy, "C_z": cz, "C_side": math.hypot(cy, cz),
+            "side_amplitude": [scale * float(np.ptp(tail[:, 2])) / 2, scale * float(np.ptp(tail[:, 3])) / 2],
+            "St": st, "St_component": "y" if comp == 2 else "z"}

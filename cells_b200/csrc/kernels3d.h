@@ -48,7 +48,7 @@ struct StepLaunch3 {
   long long N;
   int W, H, D;
   int tileTX, tileTY;  // interior tile of the step kernel: tileTY rows of tileTX cells
-  int pairTiles;       // 16-bit storage with an even width: two cells per thread
+  int pairTiles;       // f32 / 16-bit storage with an even width: two cells per thread
   int absorbX0;        // first x of the absorbing layer (W when it is off): interior tiles before
                        // it compile without the absorbing sources
   int nBody;

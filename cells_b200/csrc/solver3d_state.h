@@ -25,7 +25,7 @@ struct Cells3D : cells::HandleBase {
   int prec = 0;
   size_t bpp = 4;  // bytes per stored population
   int bx = 128, by = 1;  // interior tile of the step kernel: by rows of bx cells
-  int pairTiles = 0;     // two cells per thread (16-bit storage, even width)
+  int pairTiles = 0;     // two cells per thread (f32 or 16-bit storage, even width)
   int absorbX0 = -1;     // first x of the absorbing layer (W when there is none), from the x table
 
   void* f[2] = {nullptr, nullptr};

@@ -11,7 +11,9 @@
 //     store of a warp is one contiguous run of the SoA array f[i*N + cell]; the 19 pulls come from
 //     constant-bank bases already shifted by each direction's offset, with no flag read except in
 //     rows that hold a body cell (rowBody[]); the inlet and outlet cells of each row ride along in
-//     the same coalesced loads; 16-bit storage moves two cells per thread;
+//     the same coalesced loads; with an even width f32, f16 and bf16 storage move two cells per
+//     thread (an x-pair: one word per population for both) and collide them with packed f32x2
+//     instructions; every step grid is launched as a programmatic dependent of the previous one;
 //   * the y and z faces: the geometric boundary pull (slip mirrors, edges, outlet copy);
 //   * the body cells (every fluid cell with a flag in a row that holds a body cell): their pulls
 //     (Bouzidi walls, mirrored sources on solids) are resolved into link records when the SDF is
@@ -51,7 +53,7 @@ struct StepArgs3 {
   const float* sdf;
   const uint8_t* rowBody;
   const typename Vec4<R>::T* xTab;  // per x: (omega+ without Smagorinsky, omega-, sigma, 0)
-  // per x-pair (x0 = 2j, x0 + 1), for 16-bit storage: entry 2j (omega+ of both, omega- of both),
+  // per x-pair (x0 = 2j, x0 + 1), for f32 rates: entry 2j (omega+ of both, omega- of both),
   // entry 2j + 1 (sigma of both, 0, 0); the same values as xTab, laid out so a pair's rates load
   // as register pairs of the packed f32x2 collision
   const float4* xPair;
@@ -519,7 +521,7 @@ __device__ __forceinline__ double ramp_speed(int kind, double target, double ram
 //   [shellBlocks, + bodyBlocks)           32 body cells per block, their 19 links resolved in parallel;
 //   [shellBlocks + bodyBlocks, + tiles)   the rows y = 1 .. H-2 of planes z = 1 .. D-2 in tiles of
 //                                         tileTY rows of tileTX cells (two cells per thread for
-//                                         16-bit storage, one otherwise).
+//                                         f32 / 16-bit storage with an even width, one otherwise).
 // The face and body blocks have the lowest indices, so they are dispatched first and run beside
 // the first interior tiles. Cells a role does not own it leaves alone: in a row that holds a body
 // cell, every cell with a flag belongs to the body role. Block 0 also advances the device step

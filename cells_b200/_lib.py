@@ -130,6 +130,8 @@ def lib() -> C.CDLL:
         "cells3d_read_flags": (I, [P, P, SZ]),
         "cells3d_sample_slice": (I, [P, I, D, I, D, I, I, P]),
         "cells_copy_roofline": (I, [I, I, I, I64, I, I, C.POINTER(D)]),
+        "cells_host_alloc": (I, [SZ, C.POINTER(P)]),
+        "cells_host_free": (None, [P]),
         "cells3d_advect_tracers": (I, [P, P, P, I, D, D]),
         "cells3d_timer_start": (I, [P]),
         "cells3d_timer_stop": (I, [P, C.POINTER(C.c_float)]),
@@ -219,3 +221,21 @@ def default_config2() -> Cells2DConfig:
 
 def nan() -> float:
     return math.nan
+
+
+def pinned_empty(n: int, dtype) -> "np.ndarray":
+    """A 1-D numpy array of n elements in page-locked host memory (cells_host_alloc), freed when the
+    array and every view of it are gone. Copies between it and the device take a direct DMA."""
+    import weakref
+
+    import numpy as np
+
+    dt = np.dtype(dtype)
+    nbytes = max(1, int(n) * dt.itemsize)
+    ptr = C.c_void_p()
+    st = lib().cells_host_alloc(nbytes, C.byref(ptr))
+    if st != CELLS_OK:
+        raise CellsError(st, (lib().cells_last_error(None) or b"").decode())
+    buf = (C.c_byte * nbytes).from_address(ptr.value)
+    weakref.finalize(buf, lib().cells_host_free, ptr.value)
+    return np.frombuffer(buf, dtype=dt, count=int(n))

@@ -306,6 +306,56 @@ __global__ void set_state3_kernel(DevState3* st, int which, unsigned step, doubl
   if (which & 8) st->status = 0u;
 }
 
+// The body role's cells (fluid cells with a non-zero flag word in a row that holds a body cell), in
+// increasing index order, built on the device: one warp per row counts them, the host turns the
+// counts into offsets, and one warp per row writes its cells in x order with ballots.
+__global__ void body_count3_kernel(int W, int nRows, const uint8_t* __restrict__ rowBody,
+                                   const uint32_t* __restrict__ flags, int* __restrict__ counts) {
+  const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (row >= nRows) return;
+  int c = 0;
+  if (rowBody[row]) {
+    for (int x = lane; x < W; x += 32) {
+      const uint32_t f = flags[(long long)row * W + x];
+      c += (f != 0u && !(f & FLAG3_SOLID)) ? 1 : 0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  }
+  if (lane == 0) counts[row] = c;
+}
+
+__global__ void body_write3_kernel(int W, int nRows, const uint8_t* __restrict__ rowBody,
+                                   const uint32_t* __restrict__ flags, const int* __restrict__ offsets,
+                                   int* __restrict__ cells) {
+  const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (row >= nRows || !rowBody[row]) return;
+  int base = offsets[row];
+  for (int x0 = 0; x0 < W; x0 += 32) {
+    const int x = x0 + lane;
+    bool take = false;
+    if (x < W) {
+      const uint32_t f = flags[(long long)row * W + x];
+      take = f != 0u && !(f & FLAG3_SOLID);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (take) cells[base + __popc(m & ((1u << lane) - 1u))] = row * W + x;
+    base += __popc(m);
+  }
+}
+
+cudaError_t launch_body_count3(int W, int nRows, const uint8_t* rowBody, const uint32_t* flags, int* counts,
+                               cudaStream_t s) {
+  body_count3_kernel<<<(unsigned)((nRows * 32LL + 255) / 256), 256, 0, s>>>(W, nRows, rowBody, flags, counts);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_body_write3(int W, int nRows, const uint8_t* rowBody, const uint32_t* flags, const int* offsets,
+                               int* cells, cudaStream_t s) {
+  body_write3_kernel<<<(unsigned)((nRows * 32LL + 255) / 256), 256, 0, s>>>(W, nRows, rowBody, flags, offsets, cells);
+  return cudaGetLastError();
+}
+
 #define CELLS_DISPATCH(prec, expr)        \
   switch (prec) {                         \
     case 0: { using C = CodecF32; expr; } break; \

@@ -1,5 +1,9 @@
 #include "device.h"
 
+#include <string>
+
+#include "../../include/cells.h"
+
 #include <cstdlib>
 
 namespace cells {
@@ -89,8 +93,19 @@ void Device::h2d(void* d, const void* h, size_t bytes) {
 
 constexpr size_t kStageBytes = 2u << 20;
 
+// Whether host memory is page-locked (allocated or registered with CUDA): such memory takes a
+// direct DMA copy.
+static bool host_is_pinned(const void* h) {
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, h) != cudaSuccess) {
+    cudaGetLastError();  // clear the error of an unknown pointer
+    return false;
+  }
+  return attr.type == cudaMemoryTypeHost;
+}
+
 void Device::d2h_large(void* h, const void* d, size_t bytes) {
-  if (fake || bytes < 2 * kStageBytes) {
+  if (fake || bytes < 2 * kStageBytes || host_is_pinned(h)) {
     d2h(h, d, bytes);
     sync();
     return;
@@ -178,3 +193,25 @@ size_t Device::free_bytes() {
 }
 
 }  // namespace cells
+
+// ---------------- pinned host buffers for callers (include/cells.h) ----------------
+namespace cells {
+extern thread_local std::string g_create_error;
+}
+
+extern "C" int cells_host_alloc(size_t bytes, void** out) {
+  if (!out || bytes == 0) return CELLS_E_INVALID;
+  *out = nullptr;
+  const cudaError_t e = cudaMallocHost(out, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cells::g_create_error = std::string("cells_host_alloc: ") + cudaGetErrorString(e);
+    *out = nullptr;
+    return CELLS_E_ALLOC;
+  }
+  return CELLS_OK;
+}
+
+extern "C" void cells_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}

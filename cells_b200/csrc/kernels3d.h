@@ -78,6 +78,12 @@ struct AuxLaunch3 {
 // body-row marks (rowBody must be zeroed first).
 cudaError_t launch_flags3(int precision, const AuxLaunch3& a, const float* sdf, uint32_t* flags, uint8_t* rowBody,
                           void* fA, void* fB, const float4* mac, cudaStream_t s);
+// The body cells of the rows marked in rowBody, in increasing index order: counts per row (H * D
+// ints), then, from the host's exclusive scan of the counts, the cells themselves.
+cudaError_t launch_body_count3(int W, int nRows, const uint8_t* rowBody, const uint32_t* flags, int* counts,
+                               cudaStream_t s);
+cudaError_t launch_body_write3(int W, int nRows, const uint8_t* rowBody, const uint32_t* flags, const int* offsets,
+                               int* cells, cudaStream_t s);
 // Resolves the 18 pulls of each listed body cell into link records (run after the flags pass).
 cudaError_t launch_links3(int precision, const AuxLaunch3& a, const int* cells, int n, const uint32_t* flags,
                           const float* sdf, const BodyLinks3& L, cudaStream_t s);

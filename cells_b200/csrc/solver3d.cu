@@ -134,23 +134,30 @@ void Cells3D::write_state(int which) {
 
 // The body kernel's cells: every fluid cell with a non-zero flag in a row that holds a body cell,
 // in increasing index order (so the force reduction order is fixed).
-void Cells3D::build_body_list(const std::vector<uint8_t>& rows) {
-  std::vector<int> cells;
+void Cells3D::build_body_list() {
+  nBody = 0;
   if (!dev.fake) {
-    std::vector<uint32_t> fl((size_t)N);
-    dev.d2h_large(fl.data(), flags, (size_t)N * 4);
-    for (int z = 0; z < D; z++)
-      for (int y = 0; y < H; y++) {
-        if (!rows[(size_t)y + (size_t)H * z]) continue;
-        const size_t base = (size_t)W * ((size_t)y + (size_t)H * z);
-        for (int x = 0; x < W; x++)
-          if (fl[base + x] != 0u && !(fl[base + x] & FLAG3_SOLID)) cells.push_back((int)(base + x));
-      }
-  }
-  nBody = (int)cells.size();
-  if (nBody > 0) {
-    dev.h2d(bodyCells, cells.data(), cells.size() * sizeof(int));
+    // counts per row on the device, offsets on the host (H * D ints each way), cells on the device
+    const int nRows = H * D;
+    int* counts = (int*)scratch_buffer((size_t)nRows * 4 * 2);
+    int* offsets = counts + nRows;
+    check_cuda(launch_body_count3(W, nRows, rowBody, flags, counts, dev.stream), "body count kernel");
+    std::vector<int> c((size_t)nRows);
+    dev.d2h(c.data(), counts, (size_t)nRows * 4);
     dev.sync();
+    long long total = 0;
+    for (int r = 0; r < nRows; r++) {
+      const int k = c[(size_t)r];
+      c[(size_t)r] = (int)total;
+      total += k;
+    }
+    nBody = (int)total;
+    if (nBody > 0) {
+      dev.h2d(offsets, c.data(), (size_t)nRows * 4);
+      check_cuda(launch_body_write3(W, nRows, rowBody, flags, offsets, bodyCells, dev.stream), "body list kernel");
+      dev.launches += 2;
+      dev.sync();
+    }
   }
   if (nBody > links.cap) {
     // grow the link tables (18 links per body cell)
@@ -173,7 +180,6 @@ void Cells3D::build_body_list(const std::vector<uint8_t>& rows) {
 // rebuildFlags, src/solver3d.ts:216-228: a macro pass on the latest populations (the refill reads
 // it), then the flags pass, then the body-row map and the body cell list.
 void Cells3D::rebuild_flags() {
-  std::vector<uint8_t> rows((size_t)H * D, 0);
   if (!dev.fake) {
     AuxLaunch3 a{W, H, D, (int)N, uIn};
     a.uIn = current_uin();
@@ -181,10 +187,8 @@ void Cells3D::rebuild_flags() {
     dev.memset0(rowBody, (size_t)H * D);
     check_cuda(launch_flags3(prec, a, sdf, flags, rowBody, f[0], f[1], macro, dev.stream), "flags kernel");
     dev.launches += 2;
-    dev.d2h(rows.data(), rowBody, rows.size());
-    dev.sync();
   }
-  build_body_list(rows);
+  build_body_list();
   argGen++;  // the body list and links are baked into step graphs
 }
 

@@ -113,7 +113,7 @@ struct Cells3D : cells::HandleBase {
   void choose_launch();
   void upload_xtab();
   void rebuild_flags();
-  void build_body_list(const std::vector<uint8_t>& rows);
+  void build_body_list();
   int enqueue_step(int par, bool sample, cudaStream_t main);
   // one step from src to dst (any buffers of 19 N populations), parity par of the device state, on
   // `stream` (nullptr: the handle's stream)

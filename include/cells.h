@@ -226,6 +226,13 @@ int cells3d_mass_noalloc(const void* populations, const uint32_t* flags, int64_t
 int cells_copy_roofline(int device, int precision, int q, int64_t n_cells, int launches, int with_flags,
                         double* ms_per_launch);
 
+/* ---------------- pinned host memory (no counterpart in the reference) ----------------
+ * Page-locked host buffers for the arrays a caller passes in and reads back (SDF, macro fields,
+ * populations): copies from and into them go straight over DMA, where pageable memory takes a
+ * staged copy. Allocation is slow; allocate once and reuse. Errors: cells_last_error(NULL). */
+int cells_host_alloc(size_t bytes, void** out);
+void cells_host_free(void* p);
+
 /* ---------------- discrete adjoint (no counterpart in the reference) ----------------
  * The forward/backward pair of a differentiable run: adjoint_forward steps the solver `steps`
  * steps from its current state (exactly like cells3d_step, plus a checkpoint of the populations

@@ -430,3 +430,29 @@ def test_prepare_steps_runs_nothing_and_graphs_match():
     assert_same(s, o, True)
     assert_forces(s.readForces(), o.readForces(), 1e-9)
     s.destroy()
+
+
+def test_pinned_host_buffers_round_trip():
+    """cells_host_alloc buffers as inputs and as the readMacro destination give the same results as
+    pageable numpy arrays."""
+    from cells_b200._lib import pinned_empty
+
+    W, H, D = 32, 16, 12
+    sdf = sphere_sdf(W, H, D, 10, 8, 6, 3)
+    m = perturbed_rest3(W, H, D, 1e-4, ux=0.05)
+    out = []
+    for pinned in (False, True):
+        s = Solver3D.create(W, H, D, precision="fp32", **BASE)
+        sd, mc = sdf, m
+        if pinned:
+            sd = pinned_empty(sdf.size, np.float32)
+            sd[:] = sdf
+            mc = pinned_empty(m.size, np.float32)
+            mc[:] = m
+        s.setSdf(sd)
+        s.initField(mc)
+        s.run(20)
+        dst = pinned_empty(4 * W * H * D, np.float32) if pinned else None
+        out.append(s.readMacro(dst).copy())
+        s.destroy()
+    assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))

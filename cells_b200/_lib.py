@@ -79,6 +79,11 @@ class Cells3DAdjointSpec(C.Structure):
                 ("checkpoint_every", C.c_int32), ("component", C.c_int32), ("scale", C.c_double)]
 
 
+class CellsStar3D(C.Structure):
+    _fields_ = [("cx", C.c_double), ("cy", C.c_double), ("cz", C.c_double), ("r0", C.c_double),
+                ("coef", C.c_double * 16)]
+
+
 class CellsError(RuntimeError):
     """A failed libcells call: ``status`` is the cells_status code, the message is the library's."""
 
@@ -142,6 +147,9 @@ def lib() -> C.CDLL:
         "cells3d_adjoint_forward": (I, [P, C.POINTER(Cells3DAdjointSpec), C.POINTER(D)]),
         "cells3d_adjoint_backward": (I, [P, P, P, C.POINTER(D), P]),
         "cells3d_adjoint_release": (I, [P]),
+        "cells3d_star_sdf": (I, [P, I, I, I, C.POINTER(CellsStar3D)]),
+        "cells3d_star_coef_gradient": (I, [C.POINTER(CellsStar3D), I, I, I, P, P]),
+        "cells3d_adjoint_backward_star": (I, [P, C.POINTER(CellsStar3D), P, C.POINTER(D)]),
         "cells3d_state_size": (I, [P, C.POINTER(SZ)]),
         "cells3d_save_state": (I, [P, P, SZ]),
         "cells3d_load_state": (I, [P, P, SZ]),
@@ -239,3 +247,43 @@ def pinned_empty(n: int, dtype) -> "np.ndarray":
     buf = (C.c_byte * nbytes).from_address(ptr.value)
     weakref.finalize(buf, lib().cells_host_free, ptr.value)
     return np.frombuffer(buf, dtype=dt, count=int(n))
+
+
+def star3d(center, r0: float, coef) -> CellsStar3D:
+    """The CellsStar3D of a star body: centre (cx, cy, cz), base radius r0, 16 coefficients."""
+    st = CellsStar3D()
+    st.cx, st.cy, st.cz = (float(v) for v in center)
+    st.r0 = float(r0)
+    c = [float(v) for v in coef]
+    if len(c) != 16:
+        raise ValueError("a star body has 16 coefficients")
+    for k in range(16):
+        st.coef[k] = c[k]
+    return st
+
+
+def star_sdf(sdf, W: int, H: int, D: int, center, r0: float, coef) -> None:
+    """Stamps the star body into the float32 SDF array in place (cells3d_star_sdf)."""
+    import numpy as np
+
+    if not (isinstance(sdf, np.ndarray) and sdf.dtype == np.float32 and sdf.flags.c_contiguous
+            and sdf.size == W * H * D):
+        raise ValueError("star_sdf needs a contiguous float32 array of W*H*D values")
+    st = lib().cells3d_star_sdf(sdf.ctypes.data, W, H, D, C.byref(star3d(center, r0, coef)))
+    if st != CELLS_OK:
+        raise CellsError(st, (lib().cells_last_error(None) or b"").decode())
+
+
+def star_coef_gradient(dsdf, W: int, H: int, D: int, center, r0: float, coef) -> "np.ndarray":
+    """dJ/dcoef (16 float64) from dJ/dSDF (W*H*D float64) through cells3d_star_coef_gradient."""
+    import numpy as np
+
+    g = np.ascontiguousarray(dsdf, dtype=np.float64)
+    if g.size != W * H * D:
+        raise ValueError("dJ/dSDF needs W*H*D values")
+    out = np.zeros(16, dtype=np.float64)
+    st = lib().cells3d_star_coef_gradient(C.byref(star3d(center, r0, coef)), W, H, D, g.ctypes.data,
+                                          out.ctypes.data)
+    if st != CELLS_OK:
+        raise CellsError(st, (lib().cells_last_error(None) or b"").decode())
+    return out

@@ -17,6 +17,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import geometry as g
+from ._lib import star_coef_gradient, star_sdf
 from .rng import perturbed_rest3
 from .solver3d import Solver3D
 from .units import derive_tau
@@ -52,7 +53,7 @@ class StarDrag:
 
     def sdf(self, coef) -> np.ndarray:
         s = g.empty_sdf3(self.W, self.H, self.D)
-        g.add_star(s, self.W, self.H, self.D, *self.center, coef, self.r0)
+        star_sdf(s, self.W, self.H, self.D, self.center, self.r0, coef)
         return s
 
     def scale(self, u) -> float:
@@ -70,32 +71,19 @@ class StarDrag:
         self._J = s.adjointForward(self.steps, self.window[0], self.window[1], self.K, 0, self.scale(u))
         return self._J
 
-    def sdf_jacobian_nodes(self, nodes: np.ndarray) -> np.ndarray:
-        """dsdf/dcoef_k = -r0 Y_k(theta, phi) at the given node indices: (len(nodes), 16)."""
-        W, H = self.W, self.H
-        x = nodes % W
-        y = (nodes // W) % H
-        z = nodes // (W * H)
-        cx, cy, cz = self.center
-        dx, dy, dz = x - cx, y - cy, z - cz
-        rr = np.sqrt(dx * dx + dy * dy + dz * dz)
-        theta = np.arccos(np.clip(np.where(rr > 0, dz / np.maximum(rr, 1e-300), 1.0), -1, 1))
-        phi = np.arctan2(dy, dx)
-        return np.stack([-self.r0 * g.real_sph_harm(l, m, theta, phi) for l, m in g.SH_INDEX], axis=1)
-
     def backward(self):
-        """(dJ/dcoef (16,), dJ/du) of the last forward: the adjoint sweep, then the host chain rule."""
+        """(dJ/dcoef (16,), dJ/du) of the last forward: the adjoint sweep and the chain rule to the
+        coefficients in one library call (cells3d_adjoint_backward_star)."""
         if self._J is None:
             raise RuntimeError("backward needs a forward first")
-        return self.coefficient_gradient(self.solver.adjointBackward())
+        dcoef, du = self.solver.adjointBackwardStar(self.center, self.r0, self._coef)
+        return dcoef, du - 2.0 * self._J / self._u
 
     def coefficient_gradient(self, r):
         """(dJ/dcoef (16,), dJ/du) from the sweep's result r (Solver3D.adjointBackward): dJ/dsdf times
-        the SDF's derivative by the coefficients at the nodes the gradient touches, and dJ/du with the
+        the SDF's derivative by the coefficients (cells3d_star_coef_gradient), and dJ/du with the
         coefficient scale's own dependence on u."""
-        dsdf = r["dsdf"]
-        nodes = np.flatnonzero(dsdf)
-        dcoef = dsdf[nodes] @ self.sdf_jacobian_nodes(nodes) if nodes.size else np.zeros(16)
+        dcoef = star_coef_gradient(r["dsdf"], self.W, self.H, self.D, self.center, self.r0, self._coef)
         du = r["du"] - 2.0 * self._J / self._u
         return dcoef, du
 

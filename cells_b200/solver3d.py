@@ -15,7 +15,7 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from ._lib import check, lib
+from ._lib import check, lib, star3d
 
 HISTORY3_LEN = 8192  # src/shaders/aux3d.ts:5
 
@@ -285,6 +285,15 @@ class Solver3D:
         check(lib().cells3d_adjoint_backward(self._h, None if t is None else t.ctypes.data, dsdf.ctypes.data,
                                              C.byref(du), None if out is None else out.ctypes.data), self._h)
         return {"dsdf": dsdf, "du": du.value, "adjoint": out}
+
+    def adjointBackwardStar(self, center, r0: float, coef):
+        """The backward sweep projected onto a star body's 16 coefficients
+        (cells3d_adjoint_backward_star): (dJ/dcoef (16 float64), dJ/du_in)."""
+        out = np.zeros(16, dtype=np.float64)
+        du = C.c_double()
+        check(lib().cells3d_adjoint_backward_star(self._h, C.byref(star3d(center, r0, coef)), out.ctypes.data,
+                                                  C.byref(du)), self._h)
+        return out, du.value
 
     def adjointRelease(self) -> None:
         check(lib().cells3d_adjoint_release(self._h), self._h)

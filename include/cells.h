@@ -261,6 +261,26 @@ typedef struct {
 int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* objective);
 int cells3d_adjoint_backward(Cells3D* h, const void* terminal_adjoint, double* dJ_dsdf, double* dJ_du_in,
                              void* adjoint_out);
+/* Star-shaped body of the shape-gradient problem: r(theta, phi) = r0 (1 + sum_k coef[k] Y_k) about
+ * (cx, cy, cz), theta the polar angle from +z, phi = atan2(dy, dx), Y_k the orthonormal real
+ * spherical harmonics of degree l <= 3 in the order (l, m) = (0,0), (1,-1), (1,0), (1,1), (2,-2) ...
+ * (3,3), without the Condon-Shortley phase. Host functions; no device work.
+ *   star_sdf            stamps min(sdf, |p - c| - r(theta, phi)) over the body's bounding box
+ *                       grown by 3 cells (the margin of every shape, src/geometry3d.ts:15-27);
+ *   star_coef_gradient  dJ/dcoef_k = sum_n dJ_dsdf[n] * (-r0 Y_k(theta_n, phi_n)), the chain rule
+ *                       from adjoint_backward's dJ/dSDF to the 16 coefficients;
+ *   adjoint_backward_star  adjoint_backward followed by that projection: the shape gradient in
+ *                       coefficients and dJ/du_in (same meaning as in adjoint_backward).
+ * Errors of the first two: cells_last_error(NULL); of the third: cells_last_error(h). */
+typedef struct {
+  double cx, cy, cz, r0;
+  double coef[16];
+} CellsStar3D;
+
+int cells3d_star_sdf(float* sdf, int32_t W, int32_t H, int32_t D, const CellsStar3D* star);
+int cells3d_star_coef_gradient(const CellsStar3D* star, int32_t W, int32_t H, int32_t D, const double* dJ_dsdf,
+                               double* dJ_dcoef16);
+int cells3d_adjoint_backward_star(Cells3D* h, const CellsStar3D* star, double* dJ_dcoef16, double* dJ_du_in);
 /* Frees the recorded run's checkpoints and tables. Without it the device block holding the
  * checkpoints, the recompute buffers and the adjoint states stays with the handle after a run, and
  * the next adjoint_forward reuses it while it fits (an optimisation loop allocates it once). */

@@ -22,7 +22,12 @@
 //     partials in a fixed order into the force ring), which is deterministic, unlike the
 //     reference's atomic slot order (src/shaders/aux3d.ts:80);
 //   * the relaxation rates and absorbing strength depend on x alone (without Smagorinsky) and come
-//     from a W-entry table that the host fills with the reference's f32 arithmetic.
+//     from a W-entry table that the host fills with the reference's f32 arithmetic;
+//   * every block first asks L2 for the pull sources of the interior tile a few z planes ahead of
+//     its own (prefetch.global.L2, one 128-byte line per thread, no registers held), so the loads
+//     of the blocks that start later find their lines in L2 instead of waiting for DRAM.
+#include <algorithm>
+
 #include "kernels3d.h"
 
 // Compiled twice: the product build (FMA contraction allowed) into cells::fast, and with
@@ -71,6 +76,7 @@ struct StepArgs3 {
   int tileTX, tileTY;            // interior tile: tileTY rows of tileTX cells
   int roleZ;                     // grid z-slices holding the face and body roles
   int absorbX0;                  // first x of the absorbing layer (W when there is none)
+  int pfPlanes;                  // L2 prefetch distance in z planes of interior tiles (0: none)
   double rampTarget, rampSteps;
   R lambda, smagC2;
 };
@@ -921,6 +927,33 @@ constexpr int step_min_blocks(bool pair) {
   return pair ? 6 : (sizeof(typename C::R) == 8 ? 4 : 8);
 }
 
+// L2 prefetch of the pull sources of the interior tile at the same (x, y) tile position pfPlanes
+// z planes later: one line per thread for each 128-byte stretch of the tile's tileTY rows in each
+// of the 19 source arrays, addressed at the stretch's middle so the pull's one-element x offset
+// still names the stretch's own line. Every address is the pull source of an interior cell, inside
+// the source buffer. A hint only: it changes no result.
+template <class C>
+__device__ __forceinline__ void prefetch_tile_ahead(const StepArgs3<C>& a) {
+  using S = typename C::S;
+  constexpr int kLine = 128;
+  const int bz = blockIdx.z + a.pfPlanes;
+  if (bz < a.roleZ || bz >= (int)gridDim.z) return;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int lpr = (a.tileTX * (int)sizeof(S) + kLine - 1) / kLine;  // stretches per tile row
+  const int z = 1 + bz - a.roleZ;
+  for (int t = tid; t < Q3 * a.tileTY * lpr; t += kStepThreads) {
+    const int i = t / (a.tileTY * lpr);
+    const int rest = t - i * a.tileTY * lpr;
+    const int r = rest / lpr;
+    const int l = rest - r * lpr;
+    const int y = 1 + blockIdx.y * a.tileTY + r;
+    if (y >= a.H - 1) continue;
+    const int x = min((int)blockIdx.x * a.tileTX + l * (kLine / (int)sizeof(S)) + kLine / 2 / (int)sizeof(S), a.W - 2);
+    const S* p = a.pull[i] + (x + (long long)a.W * (y + (long long)a.H * z));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+  }
+}
+
 template <class C, bool SMAG, bool PAIR>
 __global__ void __launch_bounds__(kStepThreads, step_min_blocks<C>(PAIR))
     step3d_kernel(const __grid_constant__ StepArgs3<C> a) {
@@ -931,6 +964,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<C>(PAIR))
   // returns at once.
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (a.pfPlanes > 0) prefetch_tile_ahead<C>(a);
   // grid (tilesX, tilesY, roleZ + D - 2): the first roleZ slices of blocks hold the face and body
   // roles (dispatched first), the others the interior tiles, one z plane per slice
   if ((int)blockIdx.z < a.roleZ) {
@@ -1026,6 +1060,15 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   const int perSlice = tilesX * tilesY;
   a.roleZ = (a.shellBlocks + a.bodyBlocks + perSlice - 1) / perSlice;
   const dim3 grid(tilesX, tilesY, a.roleZ + zInterior);
+  // prefetch distance, measured on B200 at 192x96x96 and 256x128x128 (sphere tunnel, 1000 steps):
+  // 16-bit storage 4 planes (+1.5-3% and +6.5-8%), f32 1 plane (+0.5-1.5%), f64 the plane count
+  // nearest 270 tiles (+5% and +2%); farther prefetches lost to the demand loads
+  if (sizeof(S) == 2)
+    a.pfPlanes = 4;
+  else if (sizeof(S) == 4)
+    a.pfPlanes = 1;
+  else
+    a.pfPlanes = std::max(1, (270 + perSlice / 2) / perSlice);
   const dim3 block(pair ? L.tileTX / 2 : L.tileTX, kStepThreads / (pair ? L.tileTX / 2 : L.tileTX), 1);
   const bool smag = L.smagC2 > 0;
   void (*fn)(StepArgs3<C>) = nullptr;

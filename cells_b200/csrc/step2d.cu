@@ -196,22 +196,30 @@ __device__ __forceinline__ bool cell2(const Tunnel2& T, const Hot2<C>& h, typena
   bool slot = false;
   if (fl != 0u) {
     if (fl & FLAG2_SOLID) return false;
-    Geo2 g;
-    g.W = W;
-    g.H = h.H;
-    g.left = T.left;
-    g.right = T.right;
-    g.bottom = T.bottom;
-    g.top = T.top;
-    const R uLid = prm<R>(T, P2_ULID);
-    f[0] = (R)C::ld(&src[idx]);
+    // pullSlow's first rule: a direction without its flag bit is the plain pull, which load2
+    // already made (same element), so the general rules run for the flagged directions only. An
+    // inlet (outlet) cell whose only flagged directions are the three entering from outside the
+    // grid skips them altogether: Zou-He replaces those three pulls.
+    constexpr uint32_t kInletPlain = FLAG2_INLET | (1u << 1) | (1u << 5) | (1u << 8);
+    constexpr uint32_t kOutletPlain = FLAG2_OUTLET | (1u << 3) | (1u << 6) | (1u << 7);
+    if (fl != kInletPlain && fl != kOutletPlain) {
+      Geo2 g;
+      g.W = W;
+      g.H = h.H;
+      g.left = T.left;
+      g.right = T.right;
+      g.bottom = T.bottom;
+      g.top = T.top;
+      const R uLid = prm<R>(T, P2_ULID);
 #pragma unroll
-    for (int i = 1; i < Q2; i++)
-      f[i] = pull_slow2<C>(i, g, src, h.flags, T.sdf, (long long)N, x, y, (long long)idx, fl, uLid, force);
-    slot = (fl >> BIDX2_SHIFT) != 0u;
+      for (int i = 1; i < Q2; i++)
+        if (fl & (1u << i))
+          f[i] = pull_slow2<C>(i, g, src, h.flags, T.sdf, (long long)N, x, y, (long long)idx, fl, uLid, force);
+      slot = (fl >> BIDX2_SHIFT) != 0u;
+    }
     // Zou-He (populations stored shifted by w_i)
     if (fl & FLAG2_INLET) {
-      const R u = inlet_velocity2<R>(T.parabolic, uIn, g.H, y);
+      const R u = inlet_velocity2<R>(T.parabolic, uIn, h.H, y);
       const R r = (R(1) + f[0] + f[2] + f[4] + R(2) * (f[3] + f[6] + f[7])) / (R(1) - u);
       f[1] = f[3] + (R)(2.0 / 3.0) * r * u;
       f[5] = f[7] - R(0.5) * (f[2] - f[4]) + (R)(1.0 / 6.0) * r * u;

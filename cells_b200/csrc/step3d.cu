@@ -14,7 +14,10 @@
 //     the same coalesced loads; with an even width f32, f16 and bf16 storage move two cells per
 //     thread (an x-pair: one word per population for both) and collide them with packed f32x2
 //     instructions; every step grid is launched as a programmatic dependent of the previous one;
-//   * the y and z faces: the geometric boundary pull (slip mirrors, edges, outlet copy);
+//   * the y and z faces: the geometric boundary pull (slip mirrors, edges, outlet copy); with
+//     x-pairs, the face rows with one outside side run the interior pair code with per-side pull
+//     bases (the specular reflection is a pull of the mirrored population from the same plane or
+//     row), and only the four edge rows take the one-cell face code;
 //   * the body cells (every fluid cell with a flag in a row that holds a body cell): their pulls
 //     (Bouzidi walls, mirrored sources on solids) are resolved into link records when the SDF is
 //     set, so a step reads them with independent loads; on sampled steps the body blocks reduce
@@ -77,6 +80,19 @@ struct StepArgs3 {
   int roleZ;                     // grid z-slices holding the face and body roles
   int absorbX0;                  // first x of the absorbing layer (W when there is none)
   int pfPlanes;                  // L2 prefetch distance in z planes of interior tiles (0: none)
+  int pfShift, pfRowShift;       // log2 of the 128-byte stretches per tile row and of the rows
+  // x-pair face tiles (facePairs = 1): the rows with one outside side -- rows y = 1 .. H-2 of the
+  // z = 0 / z = D-1 planes (sides 0 / 1) and the y = 0 / y = H-1 rows of the planes between
+  // (sides 2 / 3), tileTY rows per tile -- take the interior pair code with per-side pull bases:
+  // fpull[side][i] + idx is the source of population i of cell idx (the slip face's specular
+  // reflection for the directions that enter from outside), and fout[side][i] the offset from it
+  // of the outlet copy's source for the directions with c_x = -1. The shell role keeps the edge
+  // rows (two outside sides).
+  const S* fpull[4][Q3];
+  int fout[4][Q3];
+  int facePairs, faceBlocks;
+  int faceZTiles;                // tiles of the two z planes: 2 tilesX tilesY
+  int faceYGroups;               // groups of tileTY rows along z per y side
   double rampTarget, rampSteps;
   R lambda, smagC2;
 };
@@ -594,7 +610,15 @@ __device__ __forceinline__ void shell_role(const StepArgs3<C>& a, int b, int tid
   const long long nzp = D >= 2 ? 2 : 1, nyr = H >= 2 ? 2 : 1;
   const long long inD = D > 2 ? D - 2 : 0;
   const long long cz = nzp * W * H, cy = nyr * W * inD;
-  if (t < cz) {
+  if (a.facePairs) {
+    // the face rows went to the x-pair face tiles: the four edge rows (y = 0 or H-1, z = 0 or D-1)
+    if (t >= 4LL * W) return;
+    const int e = (int)(t / W);
+    x = (int)(t - (long long)e * W);
+    y = (e & 1) ? H - 1 : 0;
+    z = (e & 2) ? D - 1 : 0;
+    onZ = true;
+  } else if (t < cz) {
     const long long plane = t / ((long long)W * H);
     const long long r = t - plane * W * H;
     z = plane == 0 ? 0 : D - 1;
@@ -840,33 +864,30 @@ __device__ __forceinline__ void bulk_role(const StepArgs3<C>& a, int tz) {
 // arrive as one word holding both cells' values (8 bytes for f32, 4 for 16-bit storage), the
 // others as two single-cell loads; the 19 results are stored as one word per population. Cells of
 // the pair that belong to the body role are left alone. ABS / OUT: the tile overlaps the absorbing
-// layer / holds the outlet column.
-template <class C, bool SMAG, bool ABS, bool OUT>
-__device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
+// layer / holds the outlet column. FACE: the pair lies in a face row of side `side` (see
+// StepArgs3::fpull), whose pull bases come from the per-side tables.
+template <class C, bool SMAG, bool ABS, bool OUT, bool FACE>
+__device__ __forceinline__ void pair_cells(const StepArgs3<C>& a, int x0, int y, int z, int side) {
   using R = typename C::R;
   using S = typename C::S;
-  const int x0 = blockIdx.x * a.tileTX + 2 * threadIdx.x;
-  const int y = 1 + blockIdx.y * a.tileTY + threadIdx.y;
-  const int z = 1 + tz;
   const int W = a.W, H = a.H;
-  if (x0 >= W || y >= H - 1) return;
   const int row = y + H * z;
   const int idx = x0 + W * row;
   const bool inlet0 = x0 == 0;
   const bool outlet1 = OUT && x0 + 1 == W - 1;
   const long long WH = (long long)W * H;
-  // the pulls go out before the body-row test, so they do not wait for it (every interior pull
-  // address is inside the grid; a pair of body cells discards them)
+  // the pulls go out before the body-row test, so they do not wait for it (every pull address is
+  // inside the source buffer; a pair of body cells discards them)
   typename C::Pair r[Q3];  // populations of the pair: x0 in the low half (.x), x0 + 1 in the high half
 #pragma unroll
   for (int i = 0; i < Q3; i++) {
-    const S* p = a.pull[i] + idx;
+    const S* p = (FACE ? a.fpull[side][i] : a.pull[i]) + idx;
     if (cx3(i) == 0) {
       r[i] = C::ld_pair(p);
     } else {
       int e1 = 1;
       // outlet: zero-gradient copy from (W-2, y, z) for the directions entering through x = W-1
-      if (cx3(i) == -1 && outlet1) e1 += (int)(-2 + cy3(i) * (long long)W + cz3(i) * WH);
+      if (cx3(i) == -1 && outlet1) e1 = FACE ? a.fout[side][i] : (int)(-1 + cy3(i) * (long long)W + cz3(i) * WH);
       r[i] = C::ld_pair2(p, p + e1);
     }
   }
@@ -919,6 +940,47 @@ __device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
   }
 }
 
+// The interior pairs of tile (blockIdx.x, blockIdx.y) in plane z = 1 + tz.
+template <class C, bool SMAG, bool ABS, bool OUT>
+__device__ __forceinline__ void bulk_pair_role(const StepArgs3<C>& a, int tz) {
+  const int x0 = blockIdx.x * a.tileTX + 2 * threadIdx.x;
+  const int y = 1 + blockIdx.y * a.tileTY + threadIdx.y;
+  if (x0 >= a.W || y >= a.H - 1) return;
+  pair_cells<C, SMAG, ABS, OUT, false>(a, x0, y, 1 + tz, 0);
+}
+
+// Face tile f: the first faceZTiles are the tiles of the z = 0 and z = D-1 planes (rows 1 .. H-2,
+// laid out as an interior plane), the others tileTY consecutive planes of the y = 0 / y = H-1 row.
+// The absorbing layer and the outlet column are decided per thread.
+template <class C, bool SMAG>
+__device__ __forceinline__ void face_pair_role(const StepArgs3<C>& a, int f) {
+  const int tilesX = (a.W + a.tileTX - 1) / a.tileTX;
+  int side, tx, y, z;
+  if (f < a.faceZTiles) {
+    const int perPlane = a.faceZTiles / 2;
+    side = f >= perPlane ? 1 : 0;
+    const int rem = f - side * perPlane;
+    const int ty = rem / tilesX;
+    tx = rem - ty * tilesX;
+    y = 1 + ty * a.tileTY + threadIdx.y;
+    z = side ? a.D - 1 : 0;
+    if (y >= a.H - 1) return;
+  } else {
+    f -= a.faceZTiles;
+    const int perSide = a.faceYGroups * tilesX;
+    side = f >= perSide ? 3 : 2;
+    const int rem = f - (side - 2) * perSide;
+    const int g = rem / tilesX;
+    tx = rem - g * tilesX;
+    y = side == 3 ? a.H - 1 : 0;
+    z = 1 + g * a.tileTY + threadIdx.y;
+    if (z >= a.D - 1) return;
+  }
+  const int x0 = tx * a.tileTX + 2 * threadIdx.x;
+  if (x0 >= a.W) return;
+  pair_cells<C, SMAG, true, true, true>(a, x0, y, z, side);
+}
+
 // Resident blocks per SM the register allocation must allow: 6 for x-pairs (80 registers; the
 // packed collision measured faster at 6 than at 7, 5 or 4), 8 for one f32 cell per thread (odd
 // widths), 4 for f64.
@@ -928,10 +990,11 @@ constexpr int step_min_blocks(bool pair) {
 }
 
 // L2 prefetch of the pull sources of the interior tile at the same (x, y) tile position pfPlanes
-// z planes later: one line per thread for each 128-byte stretch of the tile's tileTY rows in each
-// of the 19 source arrays, addressed at the stretch's middle so the pull's one-element x offset
-// still names the stretch's own line. Every address is the pull source of an interior cell, inside
-// the source buffer. A hint only: it changes no result.
+// z planes later: one thread per 128-byte stretch of each of the tile's rows (2^pfShift stretches
+// per row, 2^pfRowShift rows) in each of the 19 source arrays, each addressed at the stretch's
+// middle so the pull's one-element x offset still names the stretch's own line. Every address is
+// the pull source of an interior cell, inside the source buffer. A hint only: it changes no
+// result. (One bulk prefetch per row instead measured 8-10% slower.)
 template <class C>
 __device__ __forceinline__ void prefetch_tile_ahead(const StepArgs3<C>& a) {
   using S = typename C::S;
@@ -939,18 +1002,16 @@ __device__ __forceinline__ void prefetch_tile_ahead(const StepArgs3<C>& a) {
   const int bz = blockIdx.z + a.pfPlanes;
   if (bz < a.roleZ || bz >= (int)gridDim.z) return;
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-  const int lpr = (a.tileTX * (int)sizeof(S) + kLine - 1) / kLine;  // stretches per tile row
-  const int z = 1 + bz - a.roleZ;
-  for (int t = tid; t < Q3 * a.tileTY * lpr; t += kStepThreads) {
-    const int i = t / (a.tileTY * lpr);
-    const int rest = t - i * a.tileTY * lpr;
-    const int r = rest / lpr;
-    const int l = rest - r * lpr;
+  const int perDir = a.pfRowShift + a.pfShift;  // log2 of the stretches per population
+  const long long plane = (long long)a.H * (1 + bz - a.roleZ);
+  for (int t = tid; t < (Q3 << perDir); t += kStepThreads) {
+    const int i = t >> perDir;
+    const int r = (t >> a.pfShift) & ((1 << a.pfRowShift) - 1);
+    const int l = t & ((1 << a.pfShift) - 1);
     const int y = 1 + blockIdx.y * a.tileTY + r;
     if (y >= a.H - 1) continue;
     const int x = min((int)blockIdx.x * a.tileTX + l * (kLine / (int)sizeof(S)) + kLine / 2 / (int)sizeof(S), a.W - 2);
-    const S* p = a.pull[i] + (x + (long long)a.W * (y + (long long)a.H * z));
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(a.pull[i] + (x + (long long)a.W * (y + plane))));
   }
 }
 
@@ -985,6 +1046,9 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<C>(PAIR))
       shell_role<C, SMAG>(a, r, tid);
     else if (r < a.shellBlocks + a.bodyBlocks)
       body_role<C, SMAG>(a, r - a.shellBlocks, tid);
+    else if constexpr (PAIR) {
+      if (r < a.shellBlocks + a.bodyBlocks + a.faceBlocks) face_pair_role<C, SMAG>(a, r - a.shellBlocks - a.bodyBlocks);
+    }
     return;
   }
   // block-uniform choice of the code for tiles that overlap the absorbing layer or hold the outlet
@@ -1045,11 +1109,6 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   a.smagC2 = (R)L.smagC2;
   a.absorbX0 = L.absorbX0;
   // work split
-  const long long nShell = shell_cells3(L.W, L.H, L.D);
-  a.shellBlocks = (int)((nShell + kStepThreads - 1) / kStepThreads);
-  // the body role runs when there are body cells, and on sampled steps even without them (a
-  // sample of zero force is still written to the ring, as the reference's reduce pass does)
-  a.bodyBlocks = (L.nBody > 0 || L.sample) ? body_blocks3(L.nBody) : 0;
   const bool pair = sizeof(S) <= 4 && (L.W % 2) == 0 && L.tileTX >= 64 && L.pairTiles;
   if (!pair && L.tileTX > kStepThreads) return cudaErrorInvalidValue;
   a.tileTX = L.tileTX;
@@ -1058,11 +1117,41 @@ static cudaError_t launch_step3_t(const StepLaunch3& L, cudaStream_t s) {
   const int tilesY = L.H > 2 ? (L.H - 2 + L.tileTY - 1) / L.tileTY : 1;
   const int zInterior = (L.H > 2 && L.D > 2) ? L.D - 2 : 0;
   const int perSlice = tilesX * tilesY;
-  a.roleZ = (a.shellBlocks + a.bodyBlocks + perSlice - 1) / perSlice;
+  // the face rows with one outside side as x-pair tiles (the 16-bit face code spent about 10% of
+  // the step on 4% of the cells); the outlet offsets must fit an int
+  a.facePairs = (pair && L.H >= 3 && L.D >= 3 && 19LL * L.N < (1LL << 31)) ? 1 : 0;
+  a.faceZTiles = a.facePairs ? 2 * tilesX * tilesY : 0;
+  a.faceYGroups = a.facePairs ? (L.D - 2 + L.tileTY - 1) / L.tileTY : 0;
+  a.faceBlocks = a.facePairs ? a.faceZTiles + 2 * a.faceYGroups * tilesX : 0;
+  for (int side = 0; side < 4; side++) {
+    for (int i = 0; i < Q3; i++) {
+      // the slip face's specular reflection for the directions that enter from outside: the
+      // mirrored population from the same z plane (sides 0, 1) or the same y row (sides 2, 3)
+      const bool out = side == 0 ? cz3(i) == 1 : (side == 1 ? cz3(i) == -1 : (side == 2 ? cy3(i) == 1 : cy3(i) == -1));
+      const int pop = !out ? i : (side < 2 ? mirror_z3(i) : mirror_y3(i));
+      const long long off = !out ? cx3(i) + cy3(i) * W + cz3(i) * WH
+                                 : (side < 2 ? cx3(i) + cy3(i) * W : cx3(i) + cz3(i) * WH);
+      const long long base = (long long)pop * L.N - off;
+      a.fpull[side][i] = (const S*)((uintptr_t)a.src + (intptr_t)(base * (long long)sizeof(S)));
+      // the outlet copy's source of the pair's second cell, population i at (W-2, y, z), relative
+      // to its pull address
+      a.fout[side][i] = (int)((long long)i * L.N - base);
+    }
+  }
+  const long long nShell = a.facePairs ? 4LL * L.W : shell_cells3(L.W, L.H, L.D);
+  a.shellBlocks = (int)((nShell + kStepThreads - 1) / kStepThreads);
+  // the body role runs when there are body cells, and on sampled steps even without them (a
+  // sample of zero force is still written to the ring, as the reference's reduce pass does)
+  a.bodyBlocks = (L.nBody > 0 || L.sample) ? body_blocks3(L.nBody) : 0;
+  a.roleZ = (a.shellBlocks + a.bodyBlocks + a.faceBlocks + perSlice - 1) / perSlice;
   const dim3 grid(tilesX, tilesY, a.roleZ + zInterior);
   // prefetch distance, measured on B200 at 192x96x96 and 256x128x128 (sphere tunnel, 1000 steps):
   // 16-bit storage 4 planes (+1.5-3% and +6.5-8%), f32 1 plane (+0.5-1.5%), f64 the plane count
   // nearest 270 tiles (+5% and +2%); farther prefetches lost to the demand loads
+  a.pfShift = 0;
+  while ((128 << a.pfShift) < a.tileTX * (int)sizeof(S)) a.pfShift++;  // 2^shift lines hold a tile row
+  a.pfRowShift = 0;
+  while ((1 << a.pfRowShift) < a.tileTY) a.pfRowShift++;  // tileTY = 128 / block width, a power of two
   if (sizeof(S) == 2)
     a.pfPlanes = 4;
   else if (sizeof(S) == 4)

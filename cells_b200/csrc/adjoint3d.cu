@@ -14,6 +14,7 @@
 // Inflow: dJ/du_n from the inlet's feq(1, u_n) and the absorbing layer's target u_n, summed per
 // step in f64 with a fixed order.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -586,9 +587,21 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
     if (L[k].e2 >= 0) lent.push_back({L[k].e2, k, L[k].a2});
     if (L[k].cF != 0.0) lent.push_back({L[k].e1, -2, L[k].cF});
   }
-  std::vector<std::pair<long long, int>> key(lent.size());
-  for (size_t p = 0; p < lent.size(); p++) key[p] = {lent[p].e, (int)p};
-  std::sort(key.begin(), key.end());
+  // entry indices in element order, ties in insertion order: a stable LSD radix sort on the
+  // element index (below 19 N < 2^31), 8 bits a pass, as many passes as the largest element needs
+  std::vector<int> key(lent.size()), tmp(lent.size());
+  for (size_t p = 0; p < lent.size(); p++) key[p] = (int)p;
+  {
+    long long maxE = 0;
+    for (const Ent& en : lent) maxE = std::max(maxE, en.e);
+    for (int shift = 0; shift < 32 && (maxE >> shift) != 0; shift += 8) {
+      size_t count[257] = {0};
+      for (int p : key) count[(((uint32_t)lent[(size_t)p].e >> shift) & 255u) + 1]++;
+      for (int d = 0; d < 256; d++) count[d + 1] += count[d];
+      for (int p : key) tmp[count[((uint32_t)lent[(size_t)p].e >> shift) & 255u]++] = p;
+      key.swap(tmp);
+    }
+  }
   // elements without a regular reader, generated in increasing element order (direction outer)
   auto at = [&](int x, int y, int z) { return (long long)x + (long long)W * ((long long)y + (long long)H * z); };
   std::vector<std::vector<long long>> irr(Q3);  // per direction, on host threads
@@ -624,8 +637,8 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
   {
     size_t p = 0, q = 0;
     while (p < key.size() || q < irregular.size()) {
-      if (q >= irregular.size() || (p < key.size() && key[p].first <= irregular[q]))
-        ents.push_back(lent[(size_t)key[p++].second]);
+      if (q >= irregular.size() || (p < key.size() && lent[(size_t)key[p]].e <= irregular[q]))
+        ents.push_back(lent[(size_t)key[p++]]);
       else
         ents.push_back({irregular[q++], -1, 0.0});
     }
@@ -634,6 +647,12 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
   std::vector<unsigned char> rowSet;
   std::vector<int> rowStart, entLink;
   std::vector<double> entAlpha, rowPhi;
+  rowElem.reserve(ents.size());
+  rowSet.reserve(ents.size());
+  rowStart.reserve(ents.size() + 1);
+  rowPhi.reserve(ents.size());
+  entLink.reserve(lent.size());
+  entAlpha.reserve(lent.size());
   for (size_t p = 0; p < ents.size();) {
     const long long e = ents[p].e;
     unsigned char set = 0;
@@ -680,35 +699,54 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
   // per flagged cell and direction, [i][cell]: the pull's sources and coefficients, and where its
   // adjoint goes (an element index, or -(link + 1))
   const size_t ns = slow.size();
-  std::vector<int> sE1(19 * ns, 0), sE2(19 * ns, 0), sTgt(19 * ns, 0);
-  std::vector<double> sA1(19 * ns, 0.0), sA2(19 * ns, 0.0);
-  for (size_t c = 0; c < ns; c++) {
-    const int idx = slow[c];
-    const uint32_t v = fl[(size_t)idx];
-    if (v & FLAG3_INLET) continue;  // the inlet reads nothing (and has no link records)
-    const int bse = base[(size_t)idx];
-    int rank = 0;
-    for (int i = 0; i < Q3; i++) {
-      const size_t r = (size_t)i * ns + c;
-      if (i == 0 || !(v & (1u << i))) {
-        const int e = (int)(i * N + idx - off3(i, W, H));
-        sE1[r] = sE2[r] = sTgt[r] = e;
-        sA1[r] = 1.0;
-      } else {
-        const int k = bse + rank++;
-        if (bse < 0 || k >= A->nLinks) throw Error(CELLS_E_INVALID, "adjoint link table does not match the flags");
-        const AdjLink3Host& Lk = A->hostLinks[(size_t)k];
-        const bool single = Lk.e2 < 0 && Lk.a1 == 1.0;
-        // a single source with coefficient 1 is the plain index; otherwise the sign bit marks the
-        // record's two sources and coefficients
-        sE1[r] = single ? (int)Lk.e1 : (int)((uint32_t)Lk.e1 | 0x80000000u);
-        sE2[r] = Lk.e2 >= 0 ? (int)Lk.e2 : (int)Lk.e1;
-        sA1[r] = Lk.a1;
-        sA2[r] = Lk.e2 >= 0 ? Lk.a2 : 0.0;
-        sTgt[r] = -(k + 1);
+  std::vector<int> sE1(19 * ns), sE2(19 * ns), sTgt(19 * ns);
+  std::vector<double> sA1(19 * ns), sA2(19 * ns);
+  std::atomic<bool> mismatch(false);
+  // each cell's 19 records are independent: chunks of cells on host threads
+  const int TS = (int)std::min<size_t>((size_t)table_threads(), std::max<size_t>(1, ns / 4096));
+  run_threads(TS, [&](int t) {
+    for (size_t c = ns * t / TS; c < ns * (t + 1) / TS; c++) {
+      const int idx = slow[c];
+      const uint32_t v = fl[(size_t)idx];
+      if (v & FLAG3_INLET) {  // the inlet reads nothing (and has no link records)
+        for (int i = 0; i < Q3; i++) {
+          const size_t r = (size_t)i * ns + c;
+          sE1[r] = sE2[r] = sTgt[r] = 0;
+          sA1[r] = sA2[r] = 0.0;
+        }
+        continue;
+      }
+      const int bse = base[(size_t)idx];
+      int rank = 0;
+      for (int i = 0; i < Q3; i++) {
+        const size_t r = (size_t)i * ns + c;
+        sA2[r] = 0.0;
+        if (i == 0 || !(v & (1u << i))) {
+          const int e = (int)(i * N + idx - off3(i, W, H));
+          sE1[r] = sE2[r] = sTgt[r] = e;
+          sA1[r] = 1.0;
+        } else {
+          const int k = bse + rank++;
+          if (bse < 0 || k >= A->nLinks) {
+            mismatch = true;
+            sE1[r] = sE2[r] = sTgt[r] = 0;
+            sA1[r] = 0.0;
+            continue;
+          }
+          const AdjLink3Host& Lk = A->hostLinks[(size_t)k];
+          const bool single = Lk.e2 < 0 && Lk.a1 == 1.0;
+          // a single source with coefficient 1 is the plain index; otherwise the sign bit marks the
+          // record's two sources and coefficients
+          sE1[r] = single ? (int)Lk.e1 : (int)((uint32_t)Lk.e1 | 0x80000000u);
+          sE2[r] = Lk.e2 >= 0 ? (int)Lk.e2 : (int)Lk.e1;
+          sA1[r] = Lk.a1;
+          sA2[r] = Lk.e2 >= 0 ? Lk.a2 : 0.0;
+          sTgt[r] = -(k + 1);
+        }
       }
     }
-  }
+  });
+  if (mismatch) throw Error(CELLS_E_INVALID, "adjoint link table does not match the flags");
   const size_t nsr = std::max<size_t>(1, 19 * ns);
   A->sE1 = (int*)dev.alloc(nsr * 4, "adjoint flagged-cell records");
   A->sE2 = (int*)dev.alloc(nsr * 4, "adjoint flagged-cell records");
@@ -947,9 +985,32 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
   const int64_t nWin = spec->window_end - spec->window_begin + 1;
   if (nWin > HISTORY_LEN) throw Error(CELLS_E_INVALID, "the objective window exceeds the 8192-sample force ring");
   if (19ll * h->N >= (1ll << 31)) throw Error(CELLS_E_INVALID, "the adjoint supports grids of fewer than 2^31 / 19 cells");
+  // the previous run's streams, events and pinned segment slots carry over (detached here, after
+  // their work has finished, so release_adjoint keeps them)
+  Adjoint3D carry;
+  if (Adjoint3D* old = h->adj.get()) {
+    if (old->side) cudaStreamSynchronize(old->side);
+    if (old->side2) cudaStreamSynchronize(old->side2);
+    std::swap(carry.side, old->side);
+    std::swap(carry.side2, old->side2);
+    std::swap(carry.fork, old->fork);
+    std::swap(carry.join, old->join);
+    std::swap(carry.fork2, old->fork2);
+    std::swap(carry.join2, old->join2);
+    std::swap(carry.n0Host, old->n0Host);
+    std::swap(carry.n0Cap, old->n0Cap);
+  }
   release_adjoint(h);
   h->adj.reset(new Adjoint3D());
   Adjoint3D* A = h->adj.get();
+  std::swap(A->side, carry.side);
+  std::swap(A->side2, carry.side2);
+  std::swap(A->fork, carry.fork);
+  std::swap(A->join, carry.join);
+  std::swap(A->fork2, carry.fork2);
+  std::swap(A->join2, carry.join2);
+  std::swap(A->n0Host, carry.n0Host);
+  std::swap(A->n0Cap, carry.n0Cap);
   A->s0 = s0;
   A->steps = spec->steps;
   A->w0 = spec->window_begin;
@@ -1002,13 +1063,19 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
   A->uDev = (double*)dev.alloc((size_t)A->steps * 8, "adjoint step speeds");
   A->wDev = (double*)dev.alloc((size_t)A->steps * 8, "adjoint step weights");
   A->n0Dev = (int*)dev.alloc(64, "adjoint segment index");
-  A->n0Host = (int*)dev.host_pinned((size_t)nSeg * sizeof(int));
-  check_cuda(cudaStreamCreateWithFlags(&A->side, cudaStreamNonBlocking), "cudaStreamCreate");
-  check_cuda(cudaStreamCreateWithFlags(&A->side2, cudaStreamNonBlocking), "cudaStreamCreate");
-  check_cuda(cudaEventCreateWithFlags(&A->fork2, cudaEventDisableTiming), "cudaEventCreate");
-  check_cuda(cudaEventCreateWithFlags(&A->join2, cudaEventDisableTiming), "cudaEventCreate");
-  check_cuda(cudaEventCreateWithFlags(&A->fork, cudaEventDisableTiming), "cudaEventCreate");
-  check_cuda(cudaEventCreateWithFlags(&A->join, cudaEventDisableTiming), "cudaEventCreate");
+  if (A->n0Cap < (size_t)nSeg) {
+    if (A->n0Host) dev.free_host_pinned(A->n0Host);
+    A->n0Host = nullptr;
+    A->n0Cap = 0;
+    A->n0Host = (int*)dev.host_pinned((size_t)nSeg * sizeof(int));
+    A->n0Cap = (size_t)nSeg;
+  }
+  if (!A->side) check_cuda(cudaStreamCreateWithFlags(&A->side, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (!A->side2) check_cuda(cudaStreamCreateWithFlags(&A->side2, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (!A->fork2) check_cuda(cudaEventCreateWithFlags(&A->fork2, cudaEventDisableTiming), "cudaEventCreate");
+  if (!A->join2) check_cuda(cudaEventCreateWithFlags(&A->join2, cudaEventDisableTiming), "cudaEventCreate");
+  if (!A->fork) check_cuda(cudaEventCreateWithFlags(&A->fork, cudaEventDisableTiming), "cudaEventCreate");
+  if (!A->join) check_cuda(cudaEventCreateWithFlags(&A->join, cudaEventDisableTiming), "cudaEventCreate");
   // the recorded run: a checkpoint at the start of every segment, force samples in the window
   const uint64_t written0 = h->forceSamplesRead + h->forceSteps.size();
   A->uStep.resize((size_t)A->steps);

@@ -84,6 +84,7 @@ struct Adjoint3D {
   double* wDev = nullptr;    // objective weight of each recorded step (device)
   int* n0Dev = nullptr;      // first step of the segment being swept (device)
   int* n0Host = nullptr;     // pinned, one slot per segment (the source of each n0Dev copy)
+  size_t n0Cap = 0;          // slots n0Host holds
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   cudaStream_t side2 = nullptr;          // the next segment's recompute, beside the sweep

@@ -456,3 +456,34 @@ def test_pinned_host_buffers_round_trip():
         out.append(s.readMacro(dst).copy())
         s.destroy()
     assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16"])
+def test_face_pair_rows_exact(precision):
+    """Face rows as x-pair tiles: a sphere cut by the z = 0 face near the outlet and a box on the
+    y = H-1 face at the inlet, with the absorbing layer on, so the face tiles meet body rows, the
+    inlet and outlet columns and the absorbing sources."""
+    W, H, D = 24, 7, 6
+    sdf = g.empty_sdf3(W, H, D)
+    g.add_sphere(sdf, W, H, D, 19, 3, 0.5, 2.2)
+    g.add_box3(sdf, W, H, D, 2, 6, 3, 1.5, 1.2, 1.2)
+    s, o = pair(W, H, D, precision, True, sdf)
+    s.encodeSteps(12)
+    o.encodeSteps(12)
+    assert_same(s, o, True)
+    assert_forces(s.readForces(), o.readForces(), 1e-9)
+    s.destroy()
+
+
+@pytest.mark.parametrize("dims", [(20, 3, 6), (20, 6, 3), (20, 4, 4), (20, 3, 3)])
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_thin_grids_exact(dims, precision):
+    """Grids with one or two interior rows or planes: the face-pair tiles are off below three
+    cells in y or z (the face blocks then take every face row) and cover single rows above it."""
+    W, H, D = dims
+    sdf = g.empty_sdf3(W, H, D)
+    s, o = pair(W, H, D, precision, True, sdf)
+    s.encodeSteps(10)
+    o.encodeSteps(10)
+    assert_same(s, o, True)
+    s.destroy()

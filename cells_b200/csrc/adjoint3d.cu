@@ -525,17 +525,26 @@ void upload_typed(cells::Device& dev, void* d, const std::vector<double>& v) {
   dev.sync();
 }
 
+// A device buffer of the recorded run: from the handle's table block while it has room (256-byte
+// aligned), else a buffer of its own that the run frees.
+void* adj_alloc(Cells3D* h, Adjoint3D* A, size_t bytes, const char* what) {
+  bytes = (std::max<size_t>(bytes, 1) + 255) / 256 * 256;
+  A->tabNeed += bytes;
+  if (h->adjTab && A->tabUsed + bytes <= h->adjTabBytes) {
+    void* p = (char*)h->adjTab + A->tabUsed;
+    A->tabUsed += bytes;
+    return p;
+  }
+  void* p = h->dev.alloc(bytes, what);
+  A->own.push_back(p);
+  return p;
+}
+
 void release_adjoint(Cells3D* h) {
   if (!h->adj) return;
   Adjoint3D* A = h->adj.get();
-  std::vector<void*> ptrs = {A->endState, A->linkBase, A->le1, A->le2, A->la1, A->la2, A->lcF, A->lq, A->lqk,
-                             A->lamG, A->dqAcc, A->rowElem, A->rowSet, A->rowStart, A->entLink, A->entAlpha,
-                             A->rowPhi, A->blockPart, A->counter, A->dudn,
-                             A->slowCells, A->sE1, A->sE2, A->sTgt, A->sA1, A->sA2, A->ckStateBlock};
-  // the checkpoints, recompute buffers and adjoint states live in h->adjStore, which stays
-  ptrs.push_back(A->uDev);
-  ptrs.push_back(A->wDev);
-  ptrs.push_back(A->n0Dev);
+  // the checkpoints, recompute buffers and adjoint states live in h->adjStore and the tables in
+  // h->adjTab, which both stay; only the run's own buffers go
   if (!h->dev.fake) h->dev.sync();
   if (A->side) cudaStreamSynchronize(A->side);
   if (A->side2) cudaStreamSynchronize(A->side2);
@@ -549,8 +558,7 @@ void release_adjoint(Cells3D* h) {
   if (A->join) cudaEventDestroy(A->join);
   if (A->side) cudaStreamDestroy(A->side);
   if (A->n0Host) h->dev.free_host_pinned(A->n0Host);
-  for (void* p : ptrs)
-    if (p) h->dev.release(p);
+  for (void* p : A->own) h->dev.release(p);
   h->adj.reset();
 }
 
@@ -682,7 +690,7 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
       upload_typed<float>(dev, d, v);
   };
   const size_t nl = std::max<size_t>(1, L.size());
-  A->linkBase = (int*)dev.alloc((size_t)N * 4, "adjoint link base");
+  A->linkBase = (int*)adj_alloc(h, A, (size_t)N * 4, "adjoint link base");
   dev.h2d(A->linkBase, base.data(), (size_t)N * 4);
   dev.sync();
   std::vector<int> slow;
@@ -691,7 +699,7 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
     if (v != 0u && !(v & FLAG3_SOLID)) slow.push_back((int)c);
   }
   A->nSlow = (int)slow.size();
-  A->slowCells = (int*)dev.alloc(std::max<size_t>(1, slow.size()) * 4, "adjoint flagged cells");
+  A->slowCells = (int*)adj_alloc(h, A, std::max<size_t>(1, slow.size()) * 4, "adjoint flagged cells");
   if (!slow.empty()) {
     dev.h2d(A->slowCells, slow.data(), slow.size() * 4);
     dev.sync();
@@ -748,11 +756,11 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
   });
   if (mismatch) throw Error(CELLS_E_INVALID, "adjoint link table does not match the flags");
   const size_t nsr = std::max<size_t>(1, 19 * ns);
-  A->sE1 = (int*)dev.alloc(nsr * 4, "adjoint flagged-cell records");
-  A->sE2 = (int*)dev.alloc(nsr * 4, "adjoint flagged-cell records");
-  A->sTgt = (int*)dev.alloc(nsr * 4, "adjoint flagged-cell records");
-  A->sA1 = dev.alloc(nsr * (h->prec == 3 ? 8 : 4), "adjoint flagged-cell records");
-  A->sA2 = dev.alloc(nsr * (h->prec == 3 ? 8 : 4), "adjoint flagged-cell records");
+  A->sE1 = (int*)adj_alloc(h, A, nsr * 4, "adjoint flagged-cell records");
+  A->sE2 = (int*)adj_alloc(h, A, nsr * 4, "adjoint flagged-cell records");
+  A->sTgt = (int*)adj_alloc(h, A, nsr * 4, "adjoint flagged-cell records");
+  A->sA1 = adj_alloc(h, A, nsr * (h->prec == 3 ? 8 : 4), "adjoint flagged-cell records");
+  A->sA2 = adj_alloc(h, A, nsr * (h->prec == 3 ? 8 : 4), "adjoint flagged-cell records");
   if (ns) {
     dev.h2d(A->sE1, sE1.data(), sE1.size() * 4);
     dev.h2d(A->sE2, sE2.data(), sE2.size() * 4);
@@ -778,15 +786,15 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
     q[k] = L[k].q;
     qk[k] = (signed char)L[k].qKind;
   }
-  A->le1 = (long long*)dev.alloc(nl * 8, "adjoint links");
-  A->le2 = (long long*)dev.alloc(nl * 8, "adjoint links");
-  A->la1 = dev.alloc(nl * rb, "adjoint links");
-  A->la2 = dev.alloc(nl * rb, "adjoint links");
-  A->lcF = dev.alloc(nl * rb, "adjoint links");
-  A->lq = dev.alloc(nl * rb, "adjoint links");
-  A->lqk = (signed char*)dev.alloc(nl, "adjoint links");
-  A->lamG = dev.alloc(nl * rb, "adjoint link values");
-  A->dqAcc = (double*)dev.alloc(nl * 8, "adjoint dJ/dq");
+  A->le1 = (long long*)adj_alloc(h, A, nl * 8, "adjoint links");
+  A->le2 = (long long*)adj_alloc(h, A, nl * 8, "adjoint links");
+  A->la1 = adj_alloc(h, A, nl * rb, "adjoint links");
+  A->la2 = adj_alloc(h, A, nl * rb, "adjoint links");
+  A->lcF = adj_alloc(h, A, nl * rb, "adjoint links");
+  A->lq = adj_alloc(h, A, nl * rb, "adjoint links");
+  A->lqk = (signed char*)adj_alloc(h, A, nl, "adjoint links");
+  A->lamG = adj_alloc(h, A, nl * rb, "adjoint link values");
+  A->dqAcc = (double*)adj_alloc(h, A, nl * 8, "adjoint dJ/dq");
   if (!L.empty()) {
     dev.h2d(A->le1, e1.data(), L.size() * 8);
     dev.h2d(A->le2, e2.data(), L.size() * 8);
@@ -799,12 +807,12 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
   }
   const size_t nr = std::max<size_t>(1, rowElem.size());
   const size_t ne = std::max<size_t>(1, entLink.size());
-  A->rowElem = (long long*)dev.alloc(nr * 8, "adjoint rows");
-  A->rowSet = (unsigned char*)dev.alloc(nr, "adjoint rows");
-  A->rowStart = (int*)dev.alloc((nr + 1) * 4, "adjoint rows");
-  A->rowPhi = dev.alloc(nr * rb, "adjoint rows");
-  A->entLink = (int*)dev.alloc(ne * 4, "adjoint rows");
-  A->entAlpha = dev.alloc(ne * rb, "adjoint rows");
+  A->rowElem = (long long*)adj_alloc(h, A, nr * 8, "adjoint rows");
+  A->rowSet = (unsigned char*)adj_alloc(h, A, nr, "adjoint rows");
+  A->rowStart = (int*)adj_alloc(h, A, (nr + 1) * 4, "adjoint rows");
+  A->rowPhi = adj_alloc(h, A, nr * rb, "adjoint rows");
+  A->entLink = (int*)adj_alloc(h, A, ne * 4, "adjoint rows");
+  A->entAlpha = adj_alloc(h, A, ne * rb, "adjoint rows");
   if (!rowElem.empty()) {
     dev.h2d(A->rowElem, rowElem.data(), rowElem.size() * 8);
     dev.h2d(A->rowSet, rowSet.data(), rowSet.size());
@@ -988,7 +996,9 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
   // the previous run's streams, events and pinned segment slots carry over (detached here, after
   // their work has finished, so release_adjoint keeps them)
   Adjoint3D carry;
+  size_t prevNeed = 0;  // device bytes of the previous run's tables and small buffers
   if (Adjoint3D* old = h->adj.get()) {
+    prevNeed = old->tabNeed;
     if (old->side) cudaStreamSynchronize(old->side);
     if (old->side2) cudaStreamSynchronize(old->side2);
     std::swap(carry.side, old->side);
@@ -1001,6 +1011,18 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
     std::swap(carry.n0Cap, old->n0Cap);
   }
   release_adjoint(h);
+  if (prevNeed > h->adjTabBytes) {
+    // one block for the tables from now on, with room for a somewhat larger body; without the
+    // memory for it the buffers are allocated one by one as before
+    if (h->adjTab) h->dev.release(h->adjTab);
+    h->adjTab = nullptr;
+    h->adjTabBytes = 0;
+    const size_t want = prevNeed + prevNeed / 8 + ((size_t)1 << 20);
+    if (want + (size_t)h->N * 16 < h->dev.free_bytes()) {
+      h->adjTab = h->dev.alloc(want, "adjoint tables");
+      h->adjTabBytes = want;
+    }
+  }
   h->adj.reset(new Adjoint3D());
   Adjoint3D* A = h->adj.get();
   std::swap(A->side, carry.side);
@@ -1041,14 +1063,14 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
   }
   build_tables(h, A);
   char* store = (char*)h->adjStore;
-  A->ckStateBlock = (DevState3*)dev.alloc((size_t)nSeg * sizeof(DevState3), "adjoint checkpoint");
+  A->ckStateBlock = (DevState3*)adj_alloc(h, A, (size_t)nSeg * sizeof(DevState3), "adjoint checkpoint");
   for (int64_t k = 0; k < nSeg; k++) {
     A->ck.push_back(store + (size_t)k * stride);
     A->ckState.push_back(A->ckStateBlock + k);
   }
   for (int set = 0; set < 2; set++)
     for (int k = 0; k < segBufs; k++) A->seg[set].push_back(store + (size_t)(nSeg + set * segBufs + k) * stride);
-  A->endState = dev.alloc(sizeof(DevState3), "adjoint end state");
+  A->endState = adj_alloc(h, A, sizeof(DevState3), "adjoint end state");
   A->lam[0] = store + (size_t)(nSeg + 2 * segBufs) * stride;
   A->lam[1] = store + (size_t)(nSeg + 2 * segBufs + 1) * stride;
   // 32-cell x tiles: each warp still reads 128-byte rows, and the tiles before the absorbing layer
@@ -1057,12 +1079,12 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
   const int tileY = kAdjThreads / A->tileX;
   A->nBlocks = ((h->W + A->tileX - 1) / A->tileX) * ((h->H + tileY - 1) / tileY) * h->D;
   A->nParts = A->nBlocks + (A->nSlow + kSlowCells - 1) / kSlowCells;
-  A->blockPart = (double*)dev.alloc((size_t)A->nParts * 8, "adjoint partials");
-  A->counter = (unsigned*)dev.alloc(64, "adjoint counter");
-  A->dudn = (double*)dev.alloc((size_t)A->steps * 8, "adjoint du");
-  A->uDev = (double*)dev.alloc((size_t)A->steps * 8, "adjoint step speeds");
-  A->wDev = (double*)dev.alloc((size_t)A->steps * 8, "adjoint step weights");
-  A->n0Dev = (int*)dev.alloc(64, "adjoint segment index");
+  A->blockPart = (double*)adj_alloc(h, A, (size_t)A->nParts * 8, "adjoint partials");
+  A->counter = (unsigned*)adj_alloc(h, A, 64, "adjoint counter");
+  A->dudn = (double*)adj_alloc(h, A, (size_t)A->steps * 8, "adjoint du");
+  A->uDev = (double*)adj_alloc(h, A, (size_t)A->steps * 8, "adjoint step speeds");
+  A->wDev = (double*)adj_alloc(h, A, (size_t)A->steps * 8, "adjoint step weights");
+  A->n0Dev = (int*)adj_alloc(h, A, 64, "adjoint segment index");
   if (A->n0Cap < (size_t)nSeg) {
     if (A->n0Host) dev.free_host_pinned(A->n0Host);
     A->n0Host = nullptr;
@@ -1267,6 +1289,11 @@ int cells3d_adjoint_release(Cells3D* h) {
     h->dev.release(h->adjStore);
     h->adjStore = nullptr;
     h->adjStoreBytes = 0;
+  }
+  if (h->adjTab) {
+    h->dev.release(h->adjTab);
+    h->adjTab = nullptr;
+    h->adjTabBytes = 0;
   }
   ADJ_CATCH(h)
 }

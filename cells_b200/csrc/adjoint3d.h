@@ -85,6 +85,10 @@ struct Adjoint3D {
   int* n0Dev = nullptr;      // first step of the segment being swept (device)
   int* n0Host = nullptr;     // pinned, one slot per segment (the source of each n0Dev copy)
   size_t n0Cap = 0;          // slots n0Host holds
+  // device buffers of this run: carved from the handle's adjTab block while it has room (tabUsed
+  // bytes taken), else allocated on their own (own, freed with the run); tabNeed is the total
+  size_t tabUsed = 0, tabNeed = 0;
+  std::vector<void*> own;
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   cudaStream_t side2 = nullptr;          // the next segment's recompute, beside the sweep

@@ -281,9 +281,10 @@ int cells3d_star_sdf(float* sdf, int32_t W, int32_t H, int32_t D, const CellsSta
 int cells3d_star_coef_gradient(const CellsStar3D* star, int32_t W, int32_t H, int32_t D, const double* dJ_dsdf,
                                double* dJ_dcoef16);
 int cells3d_adjoint_backward_star(Cells3D* h, const CellsStar3D* star, double* dJ_dcoef16, double* dJ_du_in);
-/* Frees the recorded run's checkpoints and tables. Without it the device block holding the
- * checkpoints, the recompute buffers and the adjoint states stays with the handle after a run, and
- * the next adjoint_forward reuses it while it fits (an optimisation loop allocates it once). */
+/* Frees the recorded run's checkpoints and tables. Without it two device blocks stay with the
+ * handle after a run -- one holding the checkpoints, the recompute buffers and the adjoint states,
+ * one sized by the run for its link tables and small buffers -- and the next adjoint_forward
+ * reuses them while they fit (an optimisation loop allocates them once). */
 int cells3d_adjoint_release(Cells3D* h);
 
 /* ---------------- state save / restore (no counterpart in the reference) ----------------

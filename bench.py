@@ -481,7 +481,7 @@ def main():
         line["variants"] = [variant(prec, (W, H, D), 1000) for prec in ("fp16", "bf16", "fp64")]
         # the targets' own workload: the 256x128x128 step in FP32 and 16-bit storage, CUDA events
         big = {prec: variant(prec, (256, 128, 128), 2000) for prec in ("fp32", "fp16", "bf16")}
-        line["north_star_256x128x128"] = {
+        line["targets_256x128x128"] = {
             "workload": "D3Q19 256x128x128 sphere tunnel (d = 21.3, Re 200), 2000 timed steps after 100",
             "fp32": big["fp32"], "fp16": big["fp16"], "bf16": big["bf16"],
             "fp16_over_fp32": round(big["fp16"]["mlups"] / big["fp32"]["mlups"], 4),

@@ -981,12 +981,13 @@ __device__ __forceinline__ void face_pair_role(const StepArgs3<C>& a, int f) {
   pair_cells<C, SMAG, true, true, true>(a, x0, y, z, side);
 }
 
-// Resident blocks per SM the register allocation must allow: 6 for x-pairs (80 registers; the
-// packed collision measured faster at 6 than at 7, 5 or 4), 8 for one f32 cell per thread (odd
-// widths), 4 for f64.
+// Resident blocks per SM the register allocation must allow: 16-bit x-pairs 6 (80 registers;
+// measured faster at 6 than at 7, 5 or 4), f32 x-pairs 5 (up to 102 registers, no spills; with
+// the L2 prefetch 3.5% faster at 192x96x96 than at 6, where 68 bytes spilled), 8 for one f32 cell
+// per thread (odd widths), 4 for f64.
 template <class C>
 constexpr int step_min_blocks(bool pair) {
-  return pair ? 6 : (sizeof(typename C::R) == 8 ? 4 : 8);
+  return pair ? (sizeof(typename C::S) == 4 ? 5 : 6) : (sizeof(typename C::R) == 8 ? 4 : 8);
 }
 
 // L2 prefetch of the pull sources of the interior tile at the same (x, y) tile position pfPlanes

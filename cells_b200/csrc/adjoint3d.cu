@@ -540,6 +540,21 @@ void* adj_alloc(Cells3D* h, Adjoint3D* A, size_t bytes, const char* what) {
   return p;
 }
 
+// Makes the handle's table block hold `bytes` (with room for a somewhat larger body next time),
+// before the run has taken anything from it; without the memory for it the run's buffers are
+// allocated one by one.
+void reserve_adj_tables(Cells3D* h, Adjoint3D* A, size_t bytes) {
+  if (h->adjTabBytes >= bytes || A->tabUsed != 0) return;
+  if (h->adjTab) h->dev.release(h->adjTab);
+  h->adjTab = nullptr;
+  h->adjTabBytes = 0;
+  const size_t want = bytes + bytes / 8 + ((size_t)1 << 20);
+  if (want + (size_t)h->N * 16 < h->dev.free_bytes()) {
+    h->adjTab = h->dev.alloc(want, "adjoint tables");
+    h->adjTabBytes = want;
+  }
+}
+
 void release_adjoint(Cells3D* h) {
   if (!h->adj) return;
   Adjoint3D* A = h->adj.get();
@@ -690,14 +705,30 @@ void build_tables(Cells3D* h, Adjoint3D* A) {
       upload_typed<float>(dev, d, v);
   };
   const size_t nl = std::max<size_t>(1, L.size());
-  A->linkBase = (int*)adj_alloc(h, A, (size_t)N * 4, "adjoint link base");
-  dev.h2d(A->linkBase, base.data(), (size_t)N * 4);
-  dev.sync();
   std::vector<int> slow;
   for (long long c = 0; c < N; c++) {
     const uint32_t v = fl[(size_t)c];
     if (v != 0u && !(v & FLAG3_SOLID)) slow.push_back((int)c);
   }
+  {
+    // every device buffer of the run, as adj_alloc rounds them (these tables, then the forward
+    // run's): the handle's table block grows to hold them all before the first is taken
+    auto al = [](size_t b) { return (std::max<size_t>(b, 1) + 255) / 256 * 256; };
+    const size_t ns = slow.size(), nsr = std::max<size_t>(1, 19 * ns);
+    const size_t nr = std::max<size_t>(1, rowElem.size()), ne = std::max<size_t>(1, entLink.size());
+    const size_t nSeg = (size_t)((A->steps + A->K - 1) / A->K);
+    const int tileY = kAdjThreads / 32;
+    const size_t nBlocks = (size_t)((W + 31) / 32) * (size_t)((H + tileY - 1) / tileY) * (size_t)D;
+    const size_t nParts = nBlocks + (ns + kSlowCells - 1) / kSlowCells;
+    const size_t need = al((size_t)N * 4) + al(ns * 4) + 3 * al(nsr * 4) + 2 * al(nsr * rb) + 2 * al(nl * 8) +
+                        5 * al(nl * rb) + al(nl) + al(nl * 8) + al(nr * 8) + al(nr) + al((nr + 1) * 4) +
+                        al(nr * rb) + al(ne * 4) + al(ne * rb) + al(nSeg * sizeof(DevState3)) +
+                        al(sizeof(DevState3)) + al(nParts * 8) + 2 * al(64) + 3 * al((size_t)A->steps * 8);
+    reserve_adj_tables(h, A, need);
+  }
+  A->linkBase = (int*)adj_alloc(h, A, (size_t)N * 4, "adjoint link base");
+  dev.h2d(A->linkBase, base.data(), (size_t)N * 4);
+  dev.sync();
   A->nSlow = (int)slow.size();
   A->slowCells = (int*)adj_alloc(h, A, std::max<size_t>(1, slow.size()) * 4, "adjoint flagged cells");
   if (!slow.empty()) {
@@ -996,9 +1027,7 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
   // the previous run's streams, events and pinned segment slots carry over (detached here, after
   // their work has finished, so release_adjoint keeps them)
   Adjoint3D carry;
-  size_t prevNeed = 0;  // device bytes of the previous run's tables and small buffers
   if (Adjoint3D* old = h->adj.get()) {
-    prevNeed = old->tabNeed;
     if (old->side) cudaStreamSynchronize(old->side);
     if (old->side2) cudaStreamSynchronize(old->side2);
     std::swap(carry.side, old->side);
@@ -1011,18 +1040,6 @@ int cells3d_adjoint_forward(Cells3D* h, const Cells3DAdjointSpec* spec, double* 
     std::swap(carry.n0Cap, old->n0Cap);
   }
   release_adjoint(h);
-  if (prevNeed > h->adjTabBytes) {
-    // one block for the tables from now on, with room for a somewhat larger body; without the
-    // memory for it the buffers are allocated one by one as before
-    if (h->adjTab) h->dev.release(h->adjTab);
-    h->adjTab = nullptr;
-    h->adjTabBytes = 0;
-    const size_t want = prevNeed + prevNeed / 8 + ((size_t)1 << 20);
-    if (want + (size_t)h->N * 16 < h->dev.free_bytes()) {
-      h->adjTab = h->dev.alloc(want, "adjoint tables");
-      h->adjTabBytes = want;
-    }
-  }
   h->adj.reset(new Adjoint3D());
   Adjoint3D* A = h->adj.get();
   std::swap(A->side, carry.side);

@@ -73,8 +73,8 @@ struct Cells3D : cells::HandleBase {
   // while it fits (freed by cells3d_adjoint_release or destroy)
   void* adjStore = nullptr;
   size_t adjStoreBytes = 0;
-  // one device block for the recorded run's tables and small buffers, sized by the previous
-  // run's needs and kept for the next run while they fit
+  // one device block for the recorded run's tables and small buffers, grown to a run's needs when
+  // its tables are built and kept for the next run while they fit
   void* adjTab = nullptr;
   size_t adjTabBytes = 0;
 

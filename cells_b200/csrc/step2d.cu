@@ -448,12 +448,13 @@ __device__ __forceinline__ void tile2(const Tunnel2* __restrict__ tunnels, int t
   }
 }
 
-// The f32 kernel is latency-bound: capped at 64 registers (4 blocks of 256 threads per SM) it keeps
-// more warps resident, which measured faster than its natural 76-80 registers despite a few spilled
-// words; the f64 kernel keeps its registers.
+// Register cap of the f32 kernel (blocks of 256 threads per SM it must fit): 3 (up to 85
+// registers); measured against 4 (64 registers, a few spilled words) the batch is as fast and one
+// tunnel at a time 3% faster, while 5 and 6 (51 and 42 registers) spill and lose 12-28%. The f64
+// kernel keeps its registers.
 template <class C>
 constexpr int min_blocks2() {
-  return sizeof(typename C::R) == 4 ? 4 : 1;
+  return sizeof(typename C::R) == 4 ? 3 : 1;
 }
 
 template <class C, int ROWS>
